@@ -1,0 +1,126 @@
+"""Generate golden vectors from the reference's own CUDA code.
+
+Runs the unmodified FOR-QAOA single-device path (built into oracle/_ref by
+oracle/Makefile.ref, driven by oracle/ref_harness.cpp) on seeded inputs and
+stores inputs + outputs as .npz fixtures.  Needs a GPU; run it on a GPU host:
+
+    make -f oracle/Makefile.ref          # on a host with the reference sources
+    python tests/golden/gen_golden.py OUTDIR
+
+then copy OUTDIR/*.npz into tests/golden/.  The fixtures pin the CPU oracle
+(tests/test_oracle_golden.py) to what the reference actually computes.
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def complete_int(n, rng, lo=1, hi=10):
+    w = rng.integers(lo, hi + 1, size=(n, n)).astype(np.float64)
+    return np.triu(w, 1)
+
+
+def gnp_int(n, rng, p=0.5, lo=1, hi=10):
+    w = complete_int(n, rng, lo, hi)
+    mask = np.triu(rng.random((n, n)) < p, 1)
+    return w * mask
+
+
+def gnp_fp(n, rng, p=0.5):
+    w = np.triu(rng.random((n, n)), 1)
+    mask = np.triu(rng.random((n, n)) < p, 1)
+    return w * mask
+
+
+def regular3_fp(n, rng):
+    """Random 3-regular graph by seeded pairing with rejection, U[0,1) weights."""
+    while True:
+        stubs = np.repeat(np.arange(n), 3)
+        rng.shuffle(stubs)
+        pairs = stubs.reshape(-1, 2)
+        if np.any(pairs[:, 0] == pairs[:, 1]):
+            continue
+        a = np.minimum(pairs[:, 0], pairs[:, 1])
+        b = np.maximum(pairs[:, 0], pairs[:, 1])
+        if len(set(zip(a.tolist(), b.tolist()))) != len(a):
+            continue
+        g = np.zeros((n, n))
+        g[a, b] = rng.random(len(a))
+        return g
+
+
+def cases():
+    out = []
+    r = np.random.default_rng(20260101)
+    def ang(P):
+        return r.uniform(0, np.pi, P), r.uniform(0, np.pi / 2, P)
+    g, b = ang(3)
+    out.append(("k10_int_c3", 10, 3, complete_int(10, r), g, b, True))
+    g, b = ang(4)
+    out.append(("k12_int_c5", 12, 5, complete_int(12, r), g, b, True))
+    g, b = ang(2)
+    out.append(("k13_int_c10", 13, 10, complete_int(13, r), g, b, True))
+    g, b = ang(3)
+    out.append(("g14_fp_c7", 14, 7, gnp_fp(14, r), g, b, True))
+    # The reference CLI's own circuit: unit-weight K_N, gamma = beta = pi/4.
+    out.append(("k11_unit_pi4_c11", 11, 11, np.triu(np.ones((11, 11)), 1),
+                np.array([np.pi / 4]), np.array([np.pi / 4]), True))
+    w = r.integers(-5, 6, size=(12, 12)).astype(np.float64)
+    g, b = ang(2)
+    out.append(("k12_negint_c4", 12, 4, np.triu(w, 1), g, b, True))
+    g, b = ang(3)
+    out.append(("reg3_16_fp_c11", 16, 11, regular3_fp(16, r), g, b, False))
+    # Config 1 of the benchmark set: K_20, integer weights 1..10, p=5, C=10.
+    g, b = ang(5)
+    out.append(("k20_int_c10_p5", 20, 10, complete_int(20, r), g, b, False))
+    return out
+
+
+def run_case(name, n, C, graph, gammas, betas, full, outdir):
+    chunk = 10 if C <= 10 else 11
+    exe = os.path.join(REF_DIR, "ref_harness_c%d" % chunk)
+    P = len(gammas)
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(np.array([n, C, P], dtype=np.int32).tobytes())
+            f.write(np.ascontiguousarray(graph, dtype=np.float64).tobytes())
+            f.write(np.asarray(gammas, dtype=np.float64).tobytes())
+            f.write(np.asarray(betas, dtype=np.float64).tobytes())
+        subprocess.run([exe, fin, fout], check=True)
+        raw = np.fromfile(fout, dtype=np.uint8)
+    nb = (1 << n) * 16
+    sv = raw[:nb].view(np.complex128)
+    gfin = raw[nb:].view(np.float64).reshape(n, n)
+    rec = dict(n=n, C=C, graph=graph, gammas=np.asarray(gammas),
+               betas=np.asarray(betas), graph_final=gfin, chunk_qubit=chunk,
+               norm=np.vdot(sv, sv).real)
+    if full:
+        rec["state"] = sv
+    else:
+        rs = np.random.default_rng(7)
+        idx = np.sort(rs.choice(1 << n, size=4096, replace=False))
+        rec["sample_idx"] = idx
+        rec["sample_amp"] = sv[idx]
+        rec["abs2_sum_by_block"] = (np.abs(sv) ** 2).reshape(256, -1).sum(axis=1)
+    np.savez_compressed(os.path.join(outdir, name + ".npz"), **rec)
+    print(name, "norm", rec["norm"])
+
+
+def main():
+    outdir = sys.argv[1] if len(sys.argv) > 1 else HERE
+    os.makedirs(outdir, exist_ok=True)
+    for c in cases():
+        run_case(*c, outdir)
+
+
+if __name__ == "__main__":
+    main()
