@@ -1,0 +1,51 @@
+// fq_ctx.h -- the context object behind fq_ctx* and host-side helpers.
+#pragma once
+
+#include <vector>
+
+#include "fq_common.cuh"
+
+struct fq_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 0;
+    int ctas_per_sm = 2;  // resident pass CTAs per SM (64 KB tile each)
+    // Device scratch, allocated once at creation.
+    void* d_w = nullptr;          // N*N weights (int32 or float64)
+    double2* d_ptab = nullptr;    // integer phase table
+    double* d_partial = nullptr;  // per-CTA reduction partials
+    double* d_result = nullptr;   // small device results
+    int partial_cap = 0;
+    // Pinned host staging (uploads of weights and small tables).
+    unsigned char* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    double* h_result = nullptr;
+    cudaEvent_t stage_evt = nullptr;
+    // Graph cache: the last weights uploaded to d_w.
+    std::vector<double> g_key;
+    int g_n = -1;
+    long long launches = 0;
+};
+
+namespace fq {
+
+// Host view of a graph, prepared for the kernels.
+struct GraphPrep {
+    int N = 0;
+    bool integer = false;      // every weight an integer, cut range fits a table
+    std::vector<int> wi;       // N*N symmetric
+    std::vector<double> wd;    // N*N symmetric
+    long long W_int = 0;       // sum of weights (integer path)
+    double W = 0;              // sum of weights
+    long long cmin = 0, cmax = 0;  // range of cut values (integer path)
+};
+
+int prep_graph(const double* upper, int N, GraphPrep& g);
+// Uploads the graph's weights to ctx->d_w (skipped when unchanged).
+int upload_graph(fq_ctx* ctx, const GraphPrep& g, const double* upper);
+// Waits until the pinned staging buffer can be rewritten.
+int stage_acquire(fq_ctx* ctx);
+int validate_ctx(fq_ctx* ctx);
+
+}  // namespace fq

@@ -1,0 +1,355 @@
+// fq_pass.cuh -- the streaming tile pass every state sweep is built from.
+//
+// A pass walks the 2^N state in tiles of 2^12 amplitudes (64 KB).  A tile
+// is every amplitude whose "tile bits" vary while all other ("fixed") index
+// bits are held: tile bits 0..l-1 are physical bits 0..l-1 (contiguous rows
+// of 2^l amplitudes, for coalescing) and tile bits l..11 are physical bits
+// a..a+11-l.  With l = 12 the tile is 4096 contiguous amplitudes.  Within a
+// tile a pass can
+//   - multiply by (or, in layer 0, write) the QAOA cost phase,
+//   - apply RX to any subset of the 12 tile qubits,
+//   - accumulate <C> = sum |psi|^2 C(z),
+// so one HBM read + write covers what the reference does in separate cost,
+// RX-chunk and block-swap sweeps (src/rzz.cu:121-156, src/rx.cu:56-87,
+// src/swap.cu:76-102): high qubits are brought on chip by the strided tile
+// instead of being transposed in HBM.
+//
+// Thread layout: 256 threads x 16 amplitudes in registers.  The 16 register
+// slots of a thread are 4 tile bits; RX on those 4 qubits is register-local.
+// Three layouts rotate which 4 tile bits are register bits; moving between
+// them goes through a 64 KB shared buffer with an XOR swizzle that keeps
+// every quarter-warp's 16-byte accesses in distinct banks:
+//   L0 (load/store): regs = tile bits 8..11, lanes = 0..4,  warps = 5..7
+//   L1:              regs = tile bits 4..7,  lanes = 0..3,8, warps = 9..11
+//   L2:              regs = tile bits 0..3,  lanes = 4..8,  warps = 9..11
+//
+// Cut value of an amplitude (exact in integers for integer weights):
+//   C(z) = K(fixed) + C_TT(tile bits) + sum_{u in tile} z_u e_u(fixed)
+// with K = cut inside the fixed bits + sum_m z_m D_m, D_m = sum_{u in tile}
+// w_um, and e_u = R_u - 2 sum_m w_um z_m, R_u = sum_{m fixed} w_um.  C_TT is
+// split into the thread's 8 tile bits (constant per thread), the 4 register
+// bits (16-entry table) and their cross term (4 per-thread coefficients), so
+// each amplitude costs a few integer adds.
+#pragma once
+
+#include "fq_common.cuh"
+
+namespace fq {
+
+constexpr int kTileBits = 12;
+constexpr int kTile = 1 << kTileBits;
+constexpr int kPassThreads = 256;
+constexpr int kRegs = 16;
+constexpr int kMaxFixed = kMaxQubits - kTileBits;  // 21
+
+// Phase modes
+enum { PH_NONE = 0, PH_MUL = 1, PH_INIT = 2 };
+// Extra outputs: none, <C> partial sums, cut value of every amplitude
+enum { EX_NONE = 0, EX_ENERGY = 1, EX_DIAG = 2 };
+// Gate modes: reduced RX [[1,-it],[-it,1]] (t = tan(b/2)), reduced RX
+// [[u,-i],[-i,u]] (u = cot(b/2)), the full RX of src/rx.cu:47-50.
+enum { GM_NONE = 0, GM_TAN = 1, GM_COT = 2, GM_FULL = 3 };
+
+struct PassArgs {
+    double2* sv;
+    const void* w;        // N*N symmetric weights (int32 or float64), device
+    const double2* ptab;  // integer path: phase of cut value c at ptab[c - cmin]
+    double* partial;      // <C> partial sums, one per CTA
+    double* diag;         // cut-value output (EX_DIAG)
+    i64 ntiles;
+    int N, l, a;
+    unsigned tmask;  // RX targets among the 12 tile bits
+    int cmin, ntab;
+    double gx;       // t or u of the reduced gate
+    double c, s;     // cos, sin of angle/2 for GM_FULL
+    double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
+    double W;        // total weight
+    double scale;    // multiplies the phase
+};
+
+__device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j : a + j - l; }
+
+// Swizzled slot of tile index t in the exchange buffer.
+__device__ __forceinline__ int xslot(int t) { return t ^ ((t >> 4) & 7); }
+
+template <int GM>
+__device__ __forceinline__ void rx_pair(double2& p, double2& q, double g, double c, double s) {
+    const double2 a = p, b = q;
+    if (GM == GM_TAN) {
+        p.x = fma(g, b.y, a.x);
+        p.y = fma(-g, b.x, a.y);
+        q.x = fma(g, a.y, b.x);
+        q.y = fma(-g, a.x, b.y);
+    } else if (GM == GM_COT) {
+        p.x = fma(g, a.x, b.y);
+        p.y = fma(g, a.y, -b.x);
+        q.x = fma(g, b.x, a.y);
+        q.y = fma(g, b.y, -a.x);
+    } else {  // src/rx.cu:47-50
+        p.x = a.x * c + b.y * s;
+        p.y = a.y * c - b.x * s;
+        q.x = a.y * s + b.x * c;
+        q.y = -a.x * s + b.y * c;
+    }
+}
+
+// RX on the register bits selected by m4 (uniform across the block).
+template <int GM>
+__device__ __forceinline__ void rx_regs(double2 (&v)[kRegs], unsigned m4, double g, double c,
+                                        double s) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if ((m4 >> k) & 1u) {
+#pragma unroll
+            for (int r = 0; r < kRegs; r++)
+                if (!((r >> k) & 1)) rx_pair<GM>(v[r], v[r | (1 << k)], g, c, s);
+        }
+    }
+}
+
+// Tile index held in register r under layout L (see header comment).
+template <int L>
+__device__ __forceinline__ int lay_index(int tid, int r) {
+    const int lane = tid & 31, warp = tid >> 5;
+    if (L == 0) return tid | (r << 8);
+    if (L == 1) return (lane & 15) | ((lane >> 4) << 8) | (warp << 9) | (r << 4);
+    return (lane << 4) | (warp << 9) | r;
+}
+
+template <int LF, int LT>
+__device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid) {
+    __syncthreads();  // previous readers of buf are done
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
+}
+
+// Shared-memory bytes a pass needs for N qubits and weight type WT.
+template <typename WT>
+__host__ __device__ inline size_t pass_smem_bytes(int N) {
+    return sizeof(double2) * kTile + sizeof(double) * 8 + sizeof(int) * 24 +
+           sizeof(WT) * (N * N + 32 + 16 + 24 + 16);
+}
+
+template <typename WT, int PH, int GM, int EX, bool ST>
+__global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2* buf = reinterpret_cast<double2*>(smraw);
+    const int N = A.N, l = A.l, a = A.a;
+    const int nF = N - kTileBits;
+    double* red = reinterpret_cast<double*>(buf + kTile);  // 8 warp partials
+    int* fpos = reinterpret_cast<int*>(red + 8);           // nF fixed positions, ascending
+    WT* sw = reinterpret_cast<WT*>(fpos + 24);             // N*N weights
+    WT* ke = sw + N * N;                                   // [0] = K, [1+u] = e_u
+    WT* creg = ke + 32;                                    // 16: cut among register bits
+    WT* Dm = creg + 16;                                    // nF
+    WT* Ru = Dm + 24;                                      // 12
+    constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
+    constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
+
+    if (CUT) {
+        const WT* gw = reinterpret_cast<const WT*>(A.w);
+        for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
+        if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
+    }
+    __syncthreads();
+    if (CUT) {
+        if (tid < nF) {
+            const int m = fpos[tid];
+            WT d = 0;
+            for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
+            Dm[tid] = d;
+        } else if (tid >= 32 && tid < 32 + kTileBits) {
+            const int u = tile_phys(tid - 32, l, a);
+            WT r = 0;
+            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
+            Ru[tid - 32] = r;
+        } else if (tid >= 64 && tid < 80) {
+            const int r = tid - 64;
+            WT c = 0;
+            for (int k = 0; k < 4; k++)
+                for (int k2 = k + 1; k2 < 4; k2++)
+                    if (((r >> k) ^ (r >> k2)) & 1)
+                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
+            creg[r] = c;
+        }
+    }
+    // Per-thread constants of the cut decomposition (layout L0).
+    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
+    if (CUT) {
+        for (int j = 0; j < 8; j++) {
+            const int pj = tile_phys(j, l, a);
+            const int tj = (tid >> j) & 1;
+            for (int j2 = j + 1; j2 < 8; j2++)
+                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
+            // Edge (j, 8+k) is cut iff t_j != r_k: t_j + r_k (1 - 2 t_j).
+            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
+            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
+            if (tj) {
+                athr += w0 + w1 + w2 + w3;
+                f0 -= w0;
+                f1 -= w1;
+                f2 -= w2;
+                f3 -= w3;
+            } else {
+                f0 += w0;
+                f1 += w1;
+                f2 += w2;
+                f3 += w3;
+            }
+        }
+    }
+    // Address pieces: thread part and the 4 register-bit strides (layout L0).
+    i64 thr_off = 0;
+    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
+    const i64 rb0 = 1ll << tile_phys(8, l, a), rb1 = 1ll << tile_phys(9, l, a);
+    const i64 rb2 = 1ll << tile_phys(10, l, a), rb3 = 1ll << tile_phys(11, l, a);
+    const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
+    const bool need_l1 = (m_mid | m_lo) != 0;
+    const bool need_l2 = m_lo != 0;
+    double acc = 0, comp = 0;  // Kahan-compensated <C> accumulator
+
+    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x) {
+        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        if (CUT) {
+            __syncthreads();  // previous tile's readers of ke are done
+            if (warp == 0) {
+                WT h = 0;
+                if (lane < nF) {
+                    const int m = fpos[lane];
+                    const int zm = (int)((base >> m) & 1);
+                    if (zm) h += Dm[lane];
+                    for (int i = lane + 1; i < nF; i++)
+                        if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+                WT e = 0;
+                if (lane < kTileBits) {
+                    const int u = tile_phys(lane, l, a);
+                    e = Ru[lane];
+                    for (int i = 0; i < nF; i++)
+                        if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
+                    ke[1 + lane] = e;
+                }
+                if (lane == 0) ke[0] = h;
+            }
+            __syncthreads();
+        }
+        double2* const p = A.sv + base + thr_off;
+        double2 v[kRegs];
+        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+        if (CUT) {
+            cbase = ke[0] + athr;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if ((tid >> j) & 1) cbase += ke[1 + j];
+            g0 = f0 + ke[9];
+            g1 = f1 + ke[10];
+            g2 = f2 + ke[11];
+            g3 = f3 + ke[12];
+        }
+#pragma unroll
+        for (int r = 0; r < kRegs; r++) {
+            const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
+                            ((r & 8) ? rb3 : 0);
+            if (LOAD) v[r] = __ldcs(p + off);
+            else v[r] = make_double2(0.0, 0.0);
+        }
+        if (PH != PH_NONE) {
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                double2 ph;
+                if (sizeof(WT) == sizeof(int)) {
+                    // The cut value lies in [cmin, cmin + ntab); the clamp only
+                    // guards the table read.
+                    const int ti = min(max((int)cr - A.cmin, 0), A.ntab - 1);
+                    ph = __ldg(A.ptab + ti);
+                } else {
+                    const double S = 2.0 * (double)cr - A.W;
+                    double sn, cs;
+                    sincos(S * A.gamma / 2, &sn, &cs);
+                    ph.x = cs;
+                    ph.y = sn;
+                }
+                if (PH == PH_INIT) {
+                    v[r].x = ph.x * A.scale;
+                    v[r].y = ph.y * A.scale;
+                } else {
+                    if (sizeof(WT) != sizeof(int)) {
+                        ph.x *= A.scale;
+                        ph.y *= A.scale;
+                    }
+                    const double2 in = v[r];
+                    v[r].x = in.x * ph.x - in.y * ph.y;  // src/rzz.cu:153-154
+                    v[r].y = in.x * ph.y + in.y * ph.x;
+                }
+            }
+        }
+        if (GM != GM_NONE) {
+            rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
+            if (need_l1) {
+                exchange<0, 1>(v, buf, tid);
+                rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
+                if (need_l2) {
+                    exchange<1, 2>(v, buf, tid);
+                    rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
+                    exchange<2, 0>(v, buf, tid);
+                } else {
+                    exchange<1, 0>(v, buf, tid);
+                }
+            }
+        }
+        if (EX == EX_DIAG) {
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
+                                ((r & 8) ? rb3 : 0);
+                __stcs(A.diag + base + thr_off + off, (double)cr);
+            }
+        }
+        if (EX == EX_ENERGY) {
+            double ts = 0;
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
+            }
+            const double y = ts - comp;
+            const double t2 = acc + y;
+            comp = (t2 - acc) - y;
+            acc = t2;
+        }
+        if (ST) {
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
+                                ((r & 8) ? rb3 : 0);
+                __stcs(p + off, v[r]);
+            }
+        }
+    }
+    if (EX == EX_ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        __syncthreads();
+        if (lane == 0) red[warp] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0;
+            for (int w = 0; w < kPassThreads / 32; w++) s += red[w];
+            A.partial[blockIdx.x] = s;
+        }
+    }
+}
+
+}  // namespace fq

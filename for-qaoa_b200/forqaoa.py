@@ -1,0 +1,267 @@
+"""Python front-end of libforqaoa.so (ctypes over the C ABI in
+include/forqaoa.h).
+
+Only the C ABI is used: device memory comes from fq_state_alloc, copies go
+through fq_state_to_host / fq_state_from_host, and every call checks the
+returned status and raises FQError with the library's message.  There is no
+fallback: if libforqaoa.so is missing or fails to load, importing this module
+raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libforqaoa.so")
+
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BUSY = range(7)
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("libforqaoa.so not built: run `make -C for-qaoa_b200` "
+                      "(or __graft_entry__.build())")
+_lib = ctypes.CDLL(LIB_PATH)
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+# name -> (restype, argtypes), mirroring include/forqaoa.h
+SIGNATURES = {
+    "fq_status_string": (ctypes.c_char_p, [_i]),
+    "fq_last_error": (ctypes.c_char_p, []),
+    "fq_version": (_i, []),
+    "fq_ctx_create": (_i, [_i, _vp, ctypes.POINTER(_vp)]),
+    "fq_ctx_destroy": (_i, [_vp]),
+    "fq_ctx_synchronize": (_i, [_vp]),
+    "fq_ctx_stream": (_vp, [_vp]),
+    "fq_ctx_kernel_launches": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "fq_ctx_device_info": (_i, [_vp, _ip, _ip]),
+    "fq_state_alloc": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
+    "fq_state_free": (_i, [_vp, _vp]),
+    "fq_state_init_basis0": (_i, [_vp, _vp, _i]),
+    "fq_state_to_host": (_i, [_vp, _vp, _i, _vp]),
+    "fq_state_from_host": (_i, [_vp, _vp, _i, _vp]),
+    "fq_init_amp": (_d, [_i]),
+    "fq_cost_phase": (_i, [_vp, _vp, _i, _d, _dp, _i, _d]),
+    "fq_rx_chunk": (_i, [_vp, _vp, _i, _i, _ip, _i, _d]),
+    "fq_rx_targets": (_i, [_vp, _vp, _i, _ip, _i, _d]),
+    "fq_swap_blocks": (_i, [_vp, _vp, _i, _i, _i, _i]),
+    "fq_relabel_graph": (_i, [_dp, _i, _i, _i, _i]),
+    "fq_qaoa_forward": (_i, [_vp, _vp, _i, _i, _dp, _dp, _dp, _dp]),
+    "fq_expectation": (_i, [_vp, _vp, _i, _dp, _dp]),
+    "fq_cut_diagonal": (_i, [_vp, _vp, _i, _dp]),
+    "fq_permute_qubits": (_i, [_vp, _vp, _vp, _i, _ip]),
+    "fq_reference_label_map": (_i, [_i, _i, _i, _ip]),
+}
+for _name, (_res, _args) in SIGNATURES.items():
+    _f = getattr(_lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+class FQError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = _lib.fq_last_error().decode(errors="replace")
+        name = _lib.fq_status_string(status).decode()
+        super().__init__("%s: %s (%d): %s" % (where, name, status, msg))
+
+
+def _check(status, where):
+    if status != OK:
+        raise FQError(status, where)
+
+
+def lib():
+    return _lib
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_ip)
+
+
+def init_amp(n):
+    return _lib.fq_init_amp(n)
+
+
+def relabel_graph(graph, swap_out, swap_in, k):
+    """mapping_after_swap_conti (src/swap.cu:27-50) on a copy of graph."""
+    g = _f64(graph).copy()
+    _check(_lib.fq_relabel_graph(_dptr(g), g.shape[0], swap_out, swap_in, k),
+           "fq_relabel_graph")
+    return g
+
+
+def reference_label_map(n, C, P):
+    lab = np.zeros(n, dtype=np.int32)
+    _check(_lib.fq_reference_label_map(n, C, P, _iptr(lab)), "fq_reference_label_map")
+    return lab
+
+
+class DeviceState:
+    """2^n complex128 amplitudes in device memory owned by a Context."""
+
+    def __init__(self, ctx, n):
+        self.ctx = ctx
+        self.n = n
+        p = _vp()
+        _check(_lib.fq_state_alloc(ctx.handle, n, ctypes.byref(p)), "fq_state_alloc")
+        self.ptr = p
+
+    @property
+    def nbytes(self):
+        return 16 << self.n
+
+    def free(self):
+        if self.ptr:
+            _check(_lib.fq_state_free(self.ctx.handle, self.ptr), "fq_state_free")
+            self.ptr = None
+
+    def to_host(self, out=None):
+        if out is None:
+            out = np.empty(1 << self.n, dtype=np.complex128)
+        assert out.dtype == np.complex128 and out.flags.c_contiguous and out.size == 1 << self.n
+        _check(_lib.fq_state_to_host(self.ctx.handle, self.ptr, self.n, out.ctypes.data),
+               "fq_state_to_host")
+        return out
+
+    def from_host(self, arr):
+        a = np.ascontiguousarray(arr, dtype=np.complex128)
+        assert a.size == 1 << self.n
+        _check(_lib.fq_state_from_host(self.ctx.handle, self.ptr, self.n, a.ctypes.data),
+               "fq_state_from_host")
+        return self
+
+    def init_basis0(self):
+        _check(_lib.fq_state_init_basis0(self.ctx.handle, self.ptr, self.n),
+               "fq_state_init_basis0")
+        return self
+
+
+class Context:
+    """fq_ctx: one device, one stream, the kernels' scratch."""
+
+    def __init__(self, device=0, stream=None):
+        h = _vp()
+        _check(_lib.fq_ctx_create(device, stream, ctypes.byref(h)), "fq_ctx_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            _check(_lib.fq_ctx_destroy(self.handle), "fq_ctx_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def synchronize(self):
+        _check(_lib.fq_ctx_synchronize(self.handle), "fq_ctx_synchronize")
+
+    @property
+    def stream(self):
+        return _lib.fq_ctx_stream(self.handle)
+
+    def launches(self):
+        c = ctypes.c_longlong()
+        _check(_lib.fq_ctx_kernel_launches(self.handle, ctypes.byref(c)),
+               "fq_ctx_kernel_launches")
+        return c.value
+
+    def device_info(self):
+        a, b = _i(), _i()
+        _check(_lib.fq_ctx_device_info(self.handle, ctypes.byref(a), ctypes.byref(b)),
+               "fq_ctx_device_info")
+        return a.value, b.value
+
+    def state(self, n):
+        return DeviceState(self, n)
+
+    # -- reference-path kernels -------------------------------------------
+    def cost_phase(self, st, angle, graph, is_first, amp0=None):
+        g = _f64(graph)
+        amp0 = init_amp(st.n) if amp0 is None else amp0
+        _check(_lib.fq_cost_phase(self.handle, st.ptr, st.n, angle, _dptr(g),
+                                  int(bool(is_first)), amp0), "fq_cost_phase")
+
+    def rx_chunk(self, st, chunk_qubits, targets, angle):
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        _check(_lib.fq_rx_chunk(self.handle, st.ptr, st.n, chunk_qubits, _iptr(t), len(t),
+                                angle), "fq_rx_chunk")
+
+    def rx_targets(self, st, targets, angle):
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        _check(_lib.fq_rx_targets(self.handle, st.ptr, st.n, _iptr(t), len(t), angle),
+               "fq_rx_targets")
+
+    def swap_blocks(self, st, swap_out, swap_in, k):
+        _check(_lib.fq_swap_blocks(self.handle, st.ptr, st.n, swap_out, swap_in, k),
+               "fq_swap_blocks")
+
+    # -- fused engine --------------------------------------------------------
+    def qaoa_forward(self, st, graph, gammas, betas, energy=True):
+        g = _f64(graph)
+        ga, be = _f64(gammas), _f64(betas)
+        assert len(ga) == len(be)
+        e = np.zeros(1)
+        _check(_lib.fq_qaoa_forward(self.handle, st.ptr, st.n, len(ga), _dptr(g), _dptr(ga),
+                                    _dptr(be), _dptr(e) if energy else None),
+               "fq_qaoa_forward")
+        return float(e[0]) if energy else None
+
+    def expectation(self, st, graph):
+        g = _f64(graph)
+        e = np.zeros(1)
+        _check(_lib.fq_expectation(self.handle, st.ptr, st.n, _dptr(g), _dptr(e)),
+               "fq_expectation")
+        return float(e[0])
+
+    def cut_diagonal(self, n, graph):
+        """C(z) for every z (float64), computed on the device."""
+        g = _f64(graph)
+        tmp = DeviceState(self, n - 1) if n > 1 else DeviceState(self, 1)
+        try:
+            _check(_lib.fq_cut_diagonal(self.handle, tmp.ptr, n, _dptr(g)), "fq_cut_diagonal")
+            raw = tmp.to_host()
+        finally:
+            tmp.free()
+        return raw.view(np.float64)[: 1 << n].copy()
+
+    def permute_qubits(self, src, dst, perm):
+        p = np.ascontiguousarray(perm, dtype=np.int32)
+        _check(_lib.fq_permute_qubits(self.handle, src.ptr, dst.ptr, src.n, _iptr(p)),
+               "fq_permute_qubits")
+
+    def reference_schedule(self, st, graph, C, gammas, betas):
+        """The reference's layer loop (src/Weighted.cpp:97-138) through the
+        per-launcher entry points; returns the relabelled graph.  The state is
+        left in the reference's physical order."""
+        g = _f64(graph).copy()
+        n = st.n
+        sizes = [min(C, n - i) for i in range(0, n, C)]
+        sub0 = list(range(min(C, n)))
+        amp0 = init_amp(n)
+        for p, (ga, be) in enumerate(zip(gammas, betas)):
+            self.cost_phase(st, ga, g, p == 0, amp0)
+            swap_in = 0
+            for i, sz in enumerate(sizes):
+                self.rx_chunk(st, min(13, n), sub0[:sz], be)
+                if i < len(sizes) - 1:
+                    swap_in += sz
+                    self.swap_blocks(st, 0, swap_in, sizes[i + 1])
+                    _check(_lib.fq_relabel_graph(_dptr(g), n, 0, swap_in, sizes[i + 1]),
+                           "fq_relabel_graph")
+        return g

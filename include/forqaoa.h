@@ -1,0 +1,125 @@
+/*
+ * forqaoa.h -- C ABI of the FOR-QAOA B200 library (libforqaoa.so).
+ *
+ * A QAOA Max-Cut state-vector simulator for one NVIDIA B200 (sm_100a),
+ * written from scratch with the semantics of FOR-QAOA's single-device path
+ * (D = 0).  Every entry point takes plain pointers and sizes and returns an
+ * int status (FQ_OK = 0); nothing here exits the process.  On failure,
+ * fq_last_error() gives a message for the calling thread.
+ *
+ * Conventions (FOR-QAOA's own, see each function):
+ *  - a state is 2^N complex128 amplitudes, AoS {re, im}, in device memory;
+ *    bit q of the amplitude index is qubit q;
+ *  - a graph is an N x N row-major FP64 matrix on the HOST whose strict
+ *    upper triangle holds the edge weights, 0 = no edge (include/graph.h:
+ *    init2DGraph / addEdgeTo2DGraph, src/graph.cpp:46-64);
+ *  - cost layer: psi(z) *= exp(+i*gamma*S(z)/2), S(z) = sum over edges of
+ *    (+w if the edge is cut else -w)  (src/rzz.cu:121-156);
+ *  - mixer layer: RX(beta) = exp(-i*beta*X/2) on each qubit (src/rx.cu:32-53);
+ *  - <C> is the expected cut weight sum_z |psi(z)|^2 C(z), C = (S + W)/2.
+ * All work is asynchronous on the context's stream unless a function says
+ * it returns a host value.
+ */
+#ifndef FORQAOA_H
+#define FORQAOA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FQ_OK 0
+#define FQ_ERR_INVALID 1     /* bad argument (size, pointer, graph, angle) */
+#define FQ_ERR_UNSUPPORTED 2 /* valid in the reference but not on this path (D > 0) */
+#define FQ_ERR_CUDA 3        /* a CUDA runtime call failed */
+#define FQ_ERR_OOM 4         /* device or host memory exhausted / over budget */
+#define FQ_ERR_TIMEOUT 5     /* a bounded device-side wait gave up */
+#define FQ_ERR_BUSY 6        /* resource in use (serving admission) */
+
+typedef struct fq_ctx fq_ctx;
+
+/* ---- status / version ------------------------------------------------ */
+const char* fq_status_string(int status);
+const char* fq_last_error(void);
+int fq_version(void);
+
+/* ---- context ------------------------------------------------------------
+ * One context per (device, stream).  It owns the small device scratch used
+ * by the kernels (weights, phase tables, reduction partials) and pinned
+ * staging memory, allocated once at creation.  stream == NULL creates a
+ * private non-blocking stream (the reference's compute_stream,
+ * src/state.cpp:139). */
+int fq_ctx_create(int device, void* stream, fq_ctx** out);
+int fq_ctx_destroy(fq_ctx* ctx);
+int fq_ctx_synchronize(fq_ctx* ctx);
+void* fq_ctx_stream(fq_ctx* ctx);
+/* Number of library kernels this context has launched so far. */
+int fq_ctx_kernel_launches(fq_ctx* ctx, long long* count);
+/* Resident CTAs per SM and SM count the streaming kernels are sized for. */
+int fq_ctx_device_info(fq_ctx* ctx, int* num_sms, int* ctas_per_sm);
+
+/* ---- state memory (include/state.h, src/state.cpp) ---------------------- */
+/* cudaMalloc of 16 * 2^N bytes; replaces createState's allocation
+ * (src/state.cpp:89-159, D = 0). */
+int fq_state_alloc(fq_ctx* ctx, int N, void** sv);
+int fq_state_free(fq_ctx* ctx, void* sv);
+/* |0...0>: replaces stateInitDeviceState (src/state.cpp:198-219). */
+int fq_state_init_basis0(fq_ctx* ctx, void* sv, int N);
+/* Synchronous copies: replace stateCpyDeviceToHost / stateCpyHostToDevice
+ * (src/state.cpp:320-336). */
+int fq_state_to_host(fq_ctx* ctx, const void* sv, int N, void* host);
+int fq_state_from_host(fq_ctx* ctx, void* sv, int N, const void* host);
+
+/* ---- reference-path kernels (one per reference launcher) ---------------- */
+/* pow(1/sqrt(2), N): replaces initH (src/rzz.cu:26-28). */
+double fq_init_amp(int N);
+/* Cost layer with launch-control init: replaces rotationCompressionWeighted
+ * (src/rzz.cu:173-206, kernel :121-156).  is_first_layer != 0 writes
+ * psi = phase * init_amp without reading psi; otherwise psi *= phase. */
+int fq_cost_phase(fq_ctx* ctx, void* sv, int N, double angle,
+                  const double* graph_upper, int is_first_layer, double init_amp);
+/* RX(angle) on each of targets[0..gate_size): replaces multiRotateX
+ * (src/rx.cu:118-174).  chunk_qubits is the reference's CHUNK_QUBIT (the
+ * chunk the targets live in, 1..13); every target must be < chunk_qubits. */
+int fq_rx_chunk(fq_ctx* ctx, void* sv, int N, int chunk_qubits, const int* targets,
+                int gate_size, double angle);
+/* RX(angle) on each listed qubit, any target < N: replaces rotateX, which
+ * the reference declares (include/rx.h:25) but does not define. */
+int fq_rx_targets(fq_ctx* ctx, void* sv, int N, const int* targets, int n, double angle);
+/* Exchange qubit blocks [swap_out, swap_out+k) <-> [swap_in, swap_in+k) of
+ * every index: replaces swap_gate_conti's D = 0 path (src/swap.cu:104-202,
+ * kernel :76-102).  Requires swap_out + k <= swap_in and swap_in + k <= N. */
+int fq_swap_blocks(fq_ctx* ctx, void* sv, int N, int swap_out, int swap_in,
+                   int num_swap);
+/* Host-side graph relabel matching fq_swap_blocks: replaces
+ * mapping_after_swap_conti (src/swap.cu:27-50).  Returns a status. */
+int fq_relabel_graph(double* graph_upper, int N, int swap_out, int swap_in,
+                     int num_swap);
+
+/* ---- fused engine --------------------------------------------------------
+ * The whole P-layer circuit from |+>^N in as few HBM sweeps as possible:
+ * cost phase, launch-control init and the first 12 RX gates share one
+ * sweep, the remaining qubits are rotated in strided tiles, no block swaps.
+ * The state is left in LOGICAL qubit order.  If energy != NULL, <C> is
+ * computed in the last sweep and written to *energy (host), which
+ * synchronises the stream. */
+int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph_upper,
+                    const double* gammas, const double* betas, double* energy);
+/* <C> of a state (read-only sweep).  Writes *energy (host); synchronises. */
+int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph_upper,
+                   double* energy);
+/* Cut values C(z) for every z as float64 (exact for integer weights). */
+int fq_cut_diagonal(fq_ctx* ctx, void* out, int N, const double* graph_upper);
+/* dst[y] = src[x], y having bit perm[b] equal to bit b of x (out of place). */
+int fq_permute_qubits(fq_ctx* ctx, const void* src, void* dst, int N, const int* perm);
+/* Physical -> logical qubit map the reference schedule leaves after P layers
+ * with chunk size C (src/Weighted.cpp:97-138): label_map[b] = logical qubit
+ * at physical position b.  Host only. */
+int fq_reference_label_map(int N, int C, int P, int* label_map);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

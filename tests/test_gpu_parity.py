@@ -1,0 +1,338 @@
+"""GPU parity: every kernel entry point of the C ABI against the CPU oracle
+(seeded inputs at sizes the oracle finishes in seconds), against the golden
+vectors produced by the reference's own CUDA code, and at full sizes through
+size-independent properties."""
+import glob
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import (GOLDEN, PKG, ENERGY_RTOL, assert_state_close, complete_int, gnp_fp,
+                      gnp_int, angles)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_FILES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def rand_state(rng, n):
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+def graph_of(kind, n, rng):
+    if kind == "int":
+        return complete_int(n, rng)
+    if kind == "fp":
+        return gnp_fp(n, rng)
+    if kind == "neg":
+        return complete_int(n, rng, -5, 5)
+    if kind == "sparse":
+        return gnp_int(n, rng, 0.2)
+    raise ValueError(kind)
+
+
+# ------------------------------------------------------------ cost phase --
+
+@pytest.mark.parametrize("n", [5, 11, 12, 14, 17])
+@pytest.mark.parametrize("kind", ["int", "fp", "neg"])
+def test_cost_phase_vs_oracle(ctx, oracle, n, kind):
+    rng = np.random.default_rng(n * 7 + len(kind))
+    W = graph_of(kind, n, rng)
+    g1d = oracle.upper_tri_to_1d(W)
+    st = ctx.state(n)
+    try:
+        # layer 0: launch-control init (write-only)
+        want = np.zeros(1 << n, complex)
+        oracle.cost_phase(want, n, 0.7, g1d, True)
+        st.from_host(rand_state(rng, n))  # garbage the kernel must not read
+        ctx.cost_phase(st, 0.7, W, True)
+        assert_state_close(st.to_host(), want, what="cost init")
+        # later layer: multiply
+        v = rand_state(rng, n)
+        st.from_host(v)
+        want = v.copy()
+        oracle.cost_phase(want, n, 2.1, g1d, False)
+        ctx.cost_phase(st, 2.1, W, False)
+        assert_state_close(st.to_host(), want, what="cost mul")
+    finally:
+        st.free()
+
+
+@pytest.mark.parametrize("n", [6, 12, 15, 20])
+@pytest.mark.parametrize("kind", ["int", "neg", "fp"])
+def test_cut_diagonal_vs_oracle(ctx, oracle, n, kind):
+    rng = np.random.default_rng(n + 3)
+    W = graph_of(kind, n, rng)
+    got = ctx.cut_diagonal(n, W)
+    want = oracle.cut_values(W)
+    if kind == "fp":
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12 * max(1, W.sum()))
+    else:
+        assert np.array_equal(got, want)  # integer weights: bit-exact
+
+
+# ------------------------------------------------------------------- RX --
+
+@pytest.mark.parametrize("n,chunk,targets", [
+    (8, 8, [0, 1, 2, 3, 4, 5, 6, 7]), (12, 12, list(range(12))), (12, 10, [0, 3, 9]),
+    (14, 13, list(range(13))), (16, 13, [12, 0, 7]), (13, 13, [12]), (20, 11, [10, 2]),
+])
+def test_rx_chunk_vs_oracle(ctx, oracle, n, chunk, targets):
+    rng = np.random.default_rng(n + len(targets))
+    v = rand_state(rng, n)
+    st = ctx.state(n)
+    try:
+        st.from_host(v)
+        ctx.rx_chunk(st, chunk, targets, 1.234)
+        want = v.copy()
+        oracle.multi_rotate_x(want, n, targets, 1.234)
+        assert_state_close(st.to_host(), want, what="rx_chunk")
+    finally:
+        st.free()
+
+
+@pytest.mark.parametrize("n,targets", [(20, [0, 5, 13, 19]), (14, [13]), (9, [8, 0]),
+                                       (22, list(range(12, 22)))])
+def test_rx_targets_vs_oracle(ctx, oracle, n, targets):
+    rng = np.random.default_rng(n)
+    v = rand_state(rng, n)
+    st = ctx.state(n)
+    try:
+        st.from_host(v)
+        ctx.rx_targets(st, targets, -0.6)
+        want = v.copy()
+        oracle.multi_rotate_x(want, n, targets, -0.6)
+        assert_state_close(st.to_host(), want, what="rx_targets")
+    finally:
+        st.free()
+
+
+def test_rx_chunk_rejects_bad_targets(ctx, fq):
+    st = ctx.state(12)
+    try:
+        for chunk, t in [(10, [10]), (10, [1, 1]), (14, [0]), (10, [-1])]:
+            with pytest.raises(fq.FQError) as e:
+                ctx.rx_chunk(st, chunk, t, 0.3)
+            assert e.value.status == fq.ERR_INVALID
+    finally:
+        st.free()
+
+
+# ----------------------------------------------------------------- swap --
+
+@pytest.mark.parametrize("n,out,inn,k", [
+    (12, 0, 6, 6), (14, 0, 5, 5), (16, 2, 9, 4), (13, 0, 12, 1), (20, 0, 10, 10),
+    (18, 7, 11, 3), (20, 0, 12, 8), (15, 3, 8, 5), (22, 0, 11, 11), (21, 9, 18, 3),
+    (10, 0, 1, 1), (24, 0, 12, 12),
+])
+def test_swap_blocks_vs_oracle(ctx, oracle, n, out, inn, k):
+    rng = np.random.default_rng(n * 31 + k)
+    v = rand_state(rng, n)
+    st = ctx.state(n)
+    try:
+        st.from_host(v)
+        ctx.swap_blocks(st, out, inn, k)
+        want = v.copy()
+        oracle.swap_gate_conti(want, n, out, inn, k)
+        assert np.array_equal(st.to_host(), want)  # pure data movement: bit-exact
+    finally:
+        st.free()
+
+
+# ----------------------------------------------- reference golden vectors --
+
+def _check_golden(d, sv):
+    if "state" in d.files:
+        assert_state_close(sv, d["state"], what="vs reference output")
+    else:
+        ref = d["sample_amp"]
+        assert np.abs(sv[d["sample_idx"]] - ref).max() <= 1e-12 * np.abs(ref).max()
+        blocks = (np.abs(sv) ** 2).reshape(256, -1).sum(axis=1)
+        assert np.abs(blocks - d["abs2_sum_by_block"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("path", GOLDEN_FILES, ids=[os.path.basename(p) for p in GOLDEN_FILES])
+def test_reference_schedule_vs_golden(ctx, path):
+    """The reference's own layer loop through our per-launcher kernels
+    reproduces the reference's output, physical order and relabelled graph."""
+    d = np.load(path)
+    n = int(d["n"])
+    st = ctx.state(n)
+    try:
+        gfin = ctx.reference_schedule(st, d["graph"], int(d["C"]), d["gammas"], d["betas"])
+        _check_golden(d, st.to_host())
+        assert np.array_equal(gfin, d["graph_final"])
+    finally:
+        st.free()
+
+
+@pytest.mark.parametrize("path", GOLDEN_FILES, ids=[os.path.basename(p) for p in GOLDEN_FILES])
+def test_fused_engine_vs_golden(ctx, fq, path):
+    """The fused engine (logical order) permuted into the reference's
+    physical order reproduces the reference's output."""
+    d = np.load(path)
+    n = int(d["n"])
+    P = len(d["gammas"])
+    st, ph = ctx.state(n), ctx.state(n)
+    try:
+        ctx.qaoa_forward(st, d["graph"], d["gammas"], d["betas"], energy=False)
+        lab = fq.reference_label_map(n, int(d["C"]), P)
+        inv = np.argsort(lab)
+        ctx.permute_qubits(st, ph, inv)
+        _check_golden(d, ph.to_host())
+    finally:
+        st.free()
+        ph.free()
+
+
+# --------------------------------------------------------- fused engine --
+
+@pytest.mark.parametrize("n,P,kind", [
+    (2, 1, "int"), (3, 2, "fp"), (7, 3, "neg"), (11, 2, "int"), (12, 1, "int"), (12, 3, "fp"),
+    (13, 2, "neg"), (16, 4, "int"), (17, 2, "sparse"), (20, 3, "fp"), (21, 2, "int"),
+    (22, 2, "int"),
+])
+def test_fused_forward_vs_oracle(ctx, oracle, n, P, kind):
+    rng = np.random.default_rng(n * 13 + P)
+    W = graph_of(kind, n, rng)
+    g, b = angles(rng, P)
+    st = ctx.state(n)
+    try:
+        e = ctx.qaoa_forward(st, W, g, b, energy=True)
+        want = oracle.qaoa_logical(W, g, b)
+        assert_state_close(st.to_host(), want, what="fused forward")
+        ew = oracle.expectation(want, W)
+        assert abs(e - ew) <= ENERGY_RTOL * abs(ew)
+    finally:
+        st.free()
+
+
+@pytest.mark.parametrize("beta", [0.0, np.pi / 2 - 1e-9, 2.5, np.pi, 4.0, -1.0, 7.0])
+def test_fused_forward_mixer_angle_range(ctx, oracle, beta):
+    """Both reduced-gate forms (tan and cot) and angles outside [0, pi/2)."""
+    n, P = 14, 2
+    rng = np.random.default_rng(11)
+    W = complete_int(n, rng)
+    g = rng.uniform(0, np.pi, P)
+    b = np.array([beta, 0.3])
+    st = ctx.state(n)
+    try:
+        ctx.qaoa_forward(st, W, g, b, energy=False)
+        assert_state_close(st.to_host(), oracle.qaoa_logical(W, g, b), what="beta=%g" % beta)
+    finally:
+        st.free()
+
+
+def test_expectation_vs_oracle(ctx, oracle):
+    rng = np.random.default_rng(21)
+    for n, kind in [(9, "int"), (12, "fp"), (16, "neg"), (18, "int")]:
+        W = graph_of(kind, n, rng)
+        v = rand_state(rng, n)
+        st = ctx.state(n)
+        try:
+            st.from_host(v)
+            e = ctx.expectation(st, W)
+            ew = oracle.expectation(v, W)
+            assert abs(e - ew) <= ENERGY_RTOL * abs(ew)
+        finally:
+            st.free()
+
+
+def test_permute_qubits_vs_oracle(ctx, oracle):
+    rng = np.random.default_rng(3)
+    n = 13
+    v = rand_state(rng, n)
+    perm = rng.permutation(n)
+    a, b = ctx.state(n), ctx.state(n)
+    try:
+        a.from_host(v)
+        ctx.permute_qubits(a, b, perm)
+        assert np.array_equal(b.to_host(), oracle.permute_qubits(v, perm))
+    finally:
+        a.free()
+        b.free()
+
+
+def test_config1_k20_p5(ctx, oracle):
+    """Benchmark config 1: K_20, integer weights 1..10, p = 5, full state."""
+    rng = np.random.default_rng(2020)
+    W = complete_int(20, rng)
+    g, b = angles(rng, 5)
+    st = ctx.state(20)
+    try:
+        e = ctx.qaoa_forward(st, W, g, b)
+        want = oracle.qaoa_logical(W, g, b)
+        assert_state_close(st.to_host(), want)
+        ew = oracle.expectation(want, W)
+        assert abs(e - ew) <= ENERGY_RTOL * ew
+    finally:
+        st.free()
+
+
+# ------------------------------------------------ full-size properties --
+
+def test_kat_gamma_zero_n28(ctx):
+    """gamma = 0: RX(b)|+> = exp(-ib/2)|+>, so every amplitude equals
+    2^(-N/2) exp(-i N sum(b) / 2) exactly up to rounding."""
+    n, P = 28, 3
+    rng = np.random.default_rng(28)
+    W = complete_int(n, rng)
+    b = rng.uniform(0, np.pi / 2, P)
+    st = ctx.state(n)
+    try:
+        e = ctx.qaoa_forward(st, W, np.zeros(P), b)
+        v = st.to_host()
+        want = 2.0 ** (-n / 2) * np.exp(-1j * n * b.sum() / 2)
+        assert np.abs(v - want).max() <= 1e-12 * abs(want)
+        assert abs(e - W.sum() / 2) <= ENERGY_RTOL * W.sum()
+    finally:
+        st.free()
+
+
+def test_engines_agree_n26(ctx, fq):
+    """Two independent GPU paths at N=26: the fused engine and the reference
+    schedule (cost / RX chunks of 13 / block swaps), mapped to one order."""
+    n, P, C = 26, 3, 13
+    rng = np.random.default_rng(26)
+    W = complete_int(n, rng)
+    g, b = angles(rng, P)
+    a, r, ph = ctx.state(n), ctx.state(n), ctx.state(n)
+    try:
+        ea = ctx.qaoa_forward(a, W, g, b)
+        gfin = ctx.reference_schedule(r, W, C, g, b)
+        er = ctx.expectation(r, gfin)
+        assert abs(ea - er) <= ENERGY_RTOL * ea
+        lab = fq.reference_label_map(n, C, P)
+        ctx.permute_qubits(a, ph, np.argsort(lab))
+        assert_state_close(ph.to_host(), r.to_host(), what="fused vs reference schedule")
+    finally:
+        for s in (a, r, ph):
+            s.free()
+
+
+def test_weighted_cli_engines_agree():
+    exe = os.path.join(PKG, "weighted")
+    with tempfile.TemporaryDirectory() as td:
+        outs, es = [], []
+        for eng in ("reference", "fused"):
+            f = os.path.join(td, eng + ".bin")
+            r = subprocess.run([exe, "3", "14", "0", "5", "14", "--engine", eng, "--weights",
+                                "int", "--angles", "random", "--seed", "3", "--expect",
+                                "--dump", f], capture_output=True, text=True, timeout=120)
+            assert r.returncode == 0, r.stderr
+            assert "Total simulation time" in r.stdout
+            es.append(float(r.stdout.split("<C> :")[1].split()[0]))
+            outs.append(np.fromfile(f, dtype=np.complex128))
+        assert_state_close(outs[1], outs[0], what="CLI fused vs reference")
+        assert abs(es[0] - es[1]) <= ENERGY_RTOL * es[0]
+
+
+def test_weighted_cli_rejects_multi_device():
+    exe = os.path.join(PKG, "weighted")
+    r = subprocess.run([exe, "1", "12", "1", "4", "8"], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 1 and "D=1" in r.stderr
