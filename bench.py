@@ -1,0 +1,426 @@
+#!/usr/bin/env python3
+"""Headline benchmark: QAOA Max-Cut, N=30 qubits, p=5 layers, on B200.
+
+Workload (benchmark config 2): complete graph K_30 (435 edges) with seeded
+integer weights in 1..10, gamma_k ~ U[0,pi), beta_k ~ U[0,pi/2), complex128
+state of 2^30 amplitudes (16 GiB, far larger than the 126 MB L2, so no L2
+flush is needed between steps).  One step = the whole p=5 circuit from
+|+>^30 through the fused engine (fq_qaoa_forward).  value = layers/s over all
+ranks; every rank runs its own replica (the path has no exchange step on one
+device, so there is no data-path collective).
+
+Also reported on the same JSON line:
+  e2e          the same circuit through the public C ABI with host inputs:
+               the graph is uploaded from pinned host memory every step and
+               <C> is read back to the host every step;
+  roofline     the fused pass kernel: algorithmic bytes per launch / average
+               launch time (CUDA events on the library's stream), against the
+               measured HBM copy bandwidth;
+  cpu_baseline the oracle (plain FP64 OpenMP restatement of the reference's
+               algorithm) timed on a bounded slice of one layer on the host
+               cores, scaled to a full N=30 layer;
+  reference_schedule  the reference's own per-layer schedule (cost sweep, RX
+               chunks of C=12, block swaps) through this library's per-kernel
+               entry points, with per-kernel HBM GB/s;
+  clocks       SM clock / throttle reasons sampled during the timed region.
+
+`--impl reference` times the reference algorithm on the host cores (the
+reference ships no CPU implementation; the oracle port stands in) on the same
+workload and metric, one bounded sample per step.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "for-qaoa_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+for _p in (PKG, ORACLE_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "N=30 p=5 layers/s & HBM GB/s vs roofline; served energy+grad evals/s, p50/p99"
+UNIT = "layers/s"
+# Reference (H100, its own ncu report of `weighted 5 30 0 11 24`): 615.7 ms of
+# kernel time per layer.
+BASELINE_LAYERS_PER_S = 1.62
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--p", type=int, default=5)
+    ap.add_argument("--chunk", type=int, default=12)
+    ap.add_argument("--seed", type=int, default=30)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-ref-schedule", action="store_true")
+    ap.add_argument("--cpu-slice-bits", type=int, default=24)
+    return ap.parse_args(argv)
+
+
+def workload(n, P, seed):
+    rng = np.random.default_rng(seed)
+    graphs = [np.triu(rng.integers(1, 11, size=(n, n)).astype(np.float64), 1) for _ in range(2)]
+    gammas = rng.uniform(0, np.pi, P)
+    betas = rng.uniform(0, np.pi / 2, P)
+    return graphs, gammas, betas
+
+
+def workload_config(args):
+    return {
+        "workload": "QAOA Max-Cut N=%d p=%d, K_%d integer weights 1..10, complex128 state "
+                    "(%d GiB)" % (args.n, args.p, args.n, (16 << args.n) >> 30),
+        "N": args.n, "p": args.p, "graph": "K%d" % args.n, "weights": "int U{1..10}",
+        "angles": "gamma~U[0,pi), beta~U[0,pi/2)", "seed": args.seed,
+        "engine": "fused tile passes", "l2": "state larger than L2 (no flush needed)",
+    }
+
+
+# ------------------------------------------------------------ distributed --
+
+class Dist:
+    """Rank bookkeeping; every rank is an independent replica.  Host-side
+    gloo collectives carry only the barrier and the timing reductions."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        return self._reduce(x, "max")
+
+    def sum(self, x):
+        return self._reduce(x, "sum")
+
+    def _reduce(self, x, op):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX if op == "max" else self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------ clocks --
+
+REASON_BITS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+               0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    """Samples SM clock, power and clock-event reasons every 200 ms (read-only
+    NVML queries) while the timed region runs."""
+
+    def __init__(self, device_index):
+        self.samples = []
+        self.max_mhz = None
+        self.err = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            h = None
+            try:
+                import torch
+                uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid).encode())
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.h = h
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report why
+            self.nv = None
+            self.err = repr(e)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                try:
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except AttributeError:
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                self.samples.append((sm, pw, rs))
+            except Exception as e:
+                self.err = repr(e)
+            self._stop.wait(0.2)
+
+    def start(self):
+        if self.nv:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [],
+                    "samples": 0, "error": self.err}
+        busy = [s for s in self.samples if not (s[2] & 0x1)] or self.samples
+        reasons = set()
+        for s in busy:
+            for bit, name in REASON_BITS.items():
+                if s[2] & bit:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(s[0] for s in busy), "sm_max_mhz": self.max_mhz,
+                "power_w_max": max(s[1] for s in busy), "reasons": sorted(reasons),
+                "samples": len(busy)}
+
+
+# ------------------------------------------------------------ roofline --
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per launch of the fused pass kernel from the committed ncu
+    summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "pass_kernel_n30.md")
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+# ------------------------------------------------------------ CPU leg --
+
+def cpu_sample(graph, gamma, beta, slice_bits):
+    import oracle
+    tc, tr, full = oracle.layer_sample(graph, slice_bits, gamma, beta)
+    return full, tc + tr, oracle.num_threads()
+
+
+def cpu_baseline_obj(args, graph, gamma, beta, reps=2):
+    best = None
+    for _ in range(reps):
+        full, wall, cores = cpu_sample(graph, gamma, beta, args.cpu_slice_bits)
+        best = full if best is None else min(best, full)
+    return {"value": 1.0 / best, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "oracle (FP64 OpenMP restatement of src/rzz.cu:121-156 and "
+                      "src/rx.cu:32-53) on one layer's work units over a 2^%d-amplitude "
+                      "slice of the N=%d circuit (cost phase with the full K_%d pair loop, "
+                      "RX on the slice's %d qubits), scaled by amplitude and pair-update "
+                      "counts to a full N=%d layer; best of %d"
+                      % (args.cpu_slice_bits, args.n, args.n, args.cpu_slice_bits, args.n,
+                         reps)}
+
+
+def run_reference_impl(args):
+    """The reference algorithm on the host cores (oracle port), same metric."""
+    d = Dist()
+    if d.rank != 0:
+        d.close()
+        return
+    graphs, gammas, betas = workload(args.n, args.p, args.seed)
+    for _ in range(args.warmup):
+        cpu_sample(graphs[0], gammas[0], betas[0], args.cpu_slice_bits)
+    t_layers = []
+    wall0 = time.perf_counter()
+    cores = 1
+    for k in range(args.steps):
+        full, _, cores = cpu_sample(graphs[0], gammas[k % args.p], betas[k % args.p],
+                                    args.cpu_slice_bits)
+        t_layers.append(full)
+    wall = time.perf_counter() - wall0
+    ms_layer = 1000.0 * statistics.mean(t_layers)
+    value = 1000.0 / ms_layer
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_layer * args.p,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / BASELINE_LAYERS_PER_S,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(args), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "each step: one layer's work units on a 2^%d-amplitude "
+                                   "slice, scaled to a full N=%d layer (wall %.1f s for %d "
+                                   "steps)" % (args.cpu_slice_bits, args.n, wall, args.steps)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    d.close()
+
+
+# ------------------------------------------------------------ GPU leg --
+
+def run_ours(args):
+    import torch
+    import forqaoa
+
+    d = Dist()
+    dev = d.local_rank
+    torch.cuda.set_device(dev)
+    graphs, gammas, betas = workload(args.n, args.p, args.seed)
+    ctx = forqaoa.Context(dev)
+    st = ctx.state(args.n)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    for _ in range(args.warmup):
+        ctx.qaoa_forward(st, graphs[0], gammas, betas, energy=False)
+    ctx.synchronize()
+
+    # ---- timed region: device-resident inputs, CUDA events on ctx's stream
+    clocks = ClockSampler(dev)
+    ctx.profile_reset()
+    ctx.set_profiling(True)
+    launches0 = ctx.launches()
+    d.barrier()
+    ctx.synchronize()
+    clocks.start()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.qaoa_forward(st, graphs[0], gammas, betas, energy=False)
+    e1.record(stream)
+    ctx.synchronize()
+    clocks.stop()
+    d.barrier()
+    launches = ctx.launches() - launches0
+    ms = e0.elapsed_time(e1)
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    ms_max = d.max(ms)
+    ms_per_step = ms_max / args.steps
+    value = d.world * args.p * args.steps / (ms_max / 1000.0)
+
+    # ---- e2e: public API with host inputs (graph re-uploaded every step from
+    # pinned staging: alternate two K_30 graphs so no upload is skipped) and
+    # <C> read back to the host every step.
+    for k in range(args.warmup):
+        ctx.qaoa_forward(st, graphs[k % 2], gammas, betas, energy=True)
+    d.barrier()
+    t0 = time.perf_counter()
+    energy = None
+    for k in range(args.steps):
+        energy = ctx.qaoa_forward(st, graphs[k % 2], gammas, betas, energy=True)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = d.max(e2e_s)
+    e2e = {"value": d.world * args.p * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": 4 * args.n * args.n, "d2h_bytes_per_step": 8,
+           "ms_per_step": 1000.0 * e2e_s / args.steps, "energy_last": energy}
+
+    # ---- roofline of the fused pass kernel (both instances: layer, strided)
+    peak, peak_src = hbm_peak()
+    kern = {}
+    tot_ms = tot_b = tot_n = 0
+    for kind in ("layer_pass", "strided_pass"):
+        if kind in prof:
+            kms, kn, kb = prof[kind]
+            kern[kind] = {"launches": kn, "ms_avg": kms / kn,
+                          "alg_bytes_per_launch": kb / kn, "gbs": kb / (kms / 1000.0) / 1e9}
+            tot_ms += kms
+            tot_b += kb
+            tot_n += kn
+    achieved = tot_b / (tot_ms / 1000.0) / 1e9 if tot_ms else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if
+                peak_src == "measured" else "fallback 6.65 TB/s",
+                "traffic": ncu_traffic_per_launch(), "kernel": "fq::k_pass (fused tile pass)",
+                "alg_bytes_per_launch": (tot_b / tot_n) if tot_n else None,
+                "launches": tot_n, "per_kind": kern,
+                "kernel_share_of_step": (tot_ms / ms) if ms else None}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": value / BASELINE_LAYERS_PER_S,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+        "parallelism": "replicas" if d.world > 1 else "single",
+        "amp_updates_per_s": value * (1 << args.n) * (args.n + 1),
+        "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    st.free()
+
+    # ---- the reference's own schedule through the per-kernel entry points
+    if not args.no_ref_schedule:
+        line["reference_schedule"] = reference_schedule_leg(ctx, args, graphs[0], gammas, betas,
+                                                            peak)
+    # ---- CPU baseline (rank 0, one GPU only)
+    if not args.no_cpu and d.world == 1 and d.rank == 0:
+        line["cpu_baseline"] = cpu_baseline_obj(args, graphs[0], gammas[0], betas[0])
+    ctx.close()
+    if d.rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+
+
+def reference_schedule_leg(ctx, args, graph, gammas, betas, peak, steps=2):
+    st = ctx.state(args.n)
+    try:
+        ctx.reference_schedule(st, graph, args.chunk, gammas, betas)  # warm-up
+        ctx.synchronize()
+        ctx.profile_reset()
+        ctx.set_profiling(True)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            ctx.reference_schedule(st, graph, args.chunk, gammas, betas)
+        ctx.synchronize()
+        wall = time.perf_counter() - t0
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+    finally:
+        st.free()
+    kern_ms = sum(v[0] for v in prof.values())
+    out = {"chunk": args.chunk, "layers_per_s": args.p * steps / (kern_ms / 1000.0),
+           "wall_layers_per_s": args.p * steps / wall, "kernels": {}}
+    for kind, (kms, kn, kb) in prof.items():
+        gbs = kb / (kms / 1000.0) / 1e9 if kb else None
+        out["kernels"][kind] = {"launches": kn, "ms_avg": kms / kn, "gbs": gbs,
+                                "frac": gbs / peak if gbs else None}
+    return out
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference_impl(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

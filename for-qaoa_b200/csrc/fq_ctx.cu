@@ -27,6 +27,17 @@ int validate_ctx(fq_ctx* ctx) {
     return FQ_OK;
 }
 
+int check_device_error(fq_ctx* ctx) {
+    int flag = 0;
+    FQ_CUDA(cudaMemcpy(&flag, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        FQ_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+        set_error("a device-side bounded wait gave up (flag %d); results are incomplete", flag);
+        return FQ_ERR_TIMEOUT;
+    }
+    return FQ_OK;
+}
+
 int stage_acquire(fq_ctx* ctx) {
     FQ_CUDA(cudaEventSynchronize(ctx->stage_evt));
     return FQ_OK;
@@ -86,6 +97,52 @@ int upload_graph(fq_ctx* ctx, const GraphPrep& g, const double* upper) {
     return FQ_OK;
 }
 
+static cudaEvent_t pool_get(fq_ctx* ctx) {
+    cudaEvent_t e = nullptr;
+    if (!ctx->prof_pool.empty()) {
+        e = ctx->prof_pool.back();
+        ctx->prof_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        e = nullptr;
+    }
+    return e;
+}
+
+int prof_begin(fq_ctx* ctx) {
+    if (!ctx->profiling) return -1;
+    cudaEvent_t a = pool_get(ctx), b = pool_get(ctx);
+    if (!a || !b) return -1;
+    cudaEventRecord(a, ctx->stream);
+    ctx->prof_pending.push_back({a, b, FQ_KIND_OTHER, 0.0});
+    return (int)ctx->prof_pending.size() - 1;
+}
+
+void prof_end(fq_ctx* ctx, int token, int kind, double bytes) {
+    if (token < 0 || token >= (int)ctx->prof_pending.size()) return;
+    fq_ctx::ProfRec& r = ctx->prof_pending[token];
+    cudaEventRecord(r.b, ctx->stream);
+    r.kind = kind;
+    r.bytes = bytes;
+}
+
+static int prof_resolve(fq_ctx* ctx) {
+    if (ctx->prof_pending.empty()) return FQ_OK;
+    FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (auto& r : ctx->prof_pending) {
+        float ms = 0;
+        FQ_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        if (r.kind >= 0 && r.kind < FQ_KIND_COUNT) {
+            ctx->prof_ms[r.kind] += ms;
+            ctx->prof_bytes[r.kind] += r.bytes;
+            ctx->prof_count[r.kind]++;
+        }
+        ctx->prof_pool.push_back(r.a);
+        ctx->prof_pool.push_back(r.b);
+    }
+    ctx->prof_pending.clear();
+    return FQ_OK;
+}
+
 }  // namespace fq
 
 using namespace fq;
@@ -138,7 +195,9 @@ int fq_ctx_create(int device, void* stream, fq_ctx** out) {
         if (cudaMalloc(&c->d_w, wbytes) != cudaSuccess ||
             cudaMalloc(&c->d_ptab, sizeof(double2) * kMaxPhaseTable) != cudaSuccess ||
             cudaMalloc(&c->d_partial, sizeof(double) * c->partial_cap) != cudaSuccess ||
-            cudaMalloc(&c->d_result, sizeof(double) * 64) != cudaSuccess) {
+            cudaMalloc(&c->d_result, sizeof(double) * 64) != cudaSuccess ||
+            cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
+            cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
             st = FQ_ERR_OOM;
             break;
         }
@@ -171,9 +230,15 @@ int fq_ctx_destroy(fq_ctx* c) {
     cudaFree(c->d_ptab);
     cudaFree(c->d_partial);
     cudaFree(c->d_result);
+    cudaFree(c->d_err);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->stage_evt) cudaEventDestroy(c->stage_evt);
+    for (auto& r : c->prof_pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return FQ_OK;
@@ -182,7 +247,7 @@ int fq_ctx_destroy(fq_ctx* c) {
 int fq_ctx_synchronize(fq_ctx* ctx) {
     FQ_TRY(validate_ctx(ctx));
     FQ_CUDA(cudaStreamSynchronize(ctx->stream));
-    return FQ_OK;
+    return check_device_error(ctx);
 }
 
 void* fq_ctx_stream(fq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -190,6 +255,33 @@ void* fq_ctx_stream(fq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 int fq_ctx_kernel_launches(fq_ctx* ctx, long long* count) {
     FQ_CHECK(ctx && count, FQ_ERR_INVALID, "null argument");
     *count = ctx->launches;
+    return FQ_OK;
+}
+
+int fq_ctx_set_profiling(fq_ctx* ctx, int enable) {
+    FQ_TRY(validate_ctx(ctx));
+    ctx->profiling = enable != 0;
+    return FQ_OK;
+}
+
+int fq_ctx_profile(fq_ctx* ctx, int kind, double* total_ms, long long* launches, double* bytes) {
+    FQ_TRY(validate_ctx(ctx));
+    FQ_CHECK(kind >= 0 && kind < FQ_KIND_COUNT, FQ_ERR_INVALID, "kind %d out of range", kind);
+    FQ_TRY(prof_resolve(ctx));
+    if (total_ms) *total_ms = ctx->prof_ms[kind];
+    if (launches) *launches = ctx->prof_count[kind];
+    if (bytes) *bytes = ctx->prof_bytes[kind];
+    return FQ_OK;
+}
+
+int fq_ctx_profile_reset(fq_ctx* ctx) {
+    FQ_TRY(validate_ctx(ctx));
+    FQ_TRY(prof_resolve(ctx));
+    for (int k = 0; k < FQ_KIND_COUNT; k++) {
+        ctx->prof_ms[k] = 0;
+        ctx->prof_bytes[k] = 0;
+        ctx->prof_count[k] = 0;
+    }
     return FQ_OK;
 }
 
@@ -239,7 +331,7 @@ int fq_state_to_host(fq_ctx* ctx, const void* sv, int N, void* host) {
     FQ_CHECK(sv && host && N >= 1 && N <= kMaxQubits, FQ_ERR_INVALID, "bad arguments");
     FQ_CUDA(cudaMemcpyAsync(host, sv, sizeof(double2) << N, cudaMemcpyDeviceToHost, ctx->stream));
     FQ_CUDA(cudaStreamSynchronize(ctx->stream));
-    return FQ_OK;
+    return check_device_error(ctx);
 }
 
 int fq_state_from_host(fq_ctx* ctx, void* sv, int N, const void* host) {

@@ -16,6 +16,7 @@ struct fq_ctx {
     double2* d_ptab = nullptr;    // integer phase table
     double* d_partial = nullptr;  // per-CTA reduction partials
     double* d_result = nullptr;   // small device results
+    int* d_err = nullptr;         // kernels' error flag (nonzero: a bounded wait gave up)
     int partial_cap = 0;
     // Pinned host staging (uploads of weights and small tables).
     unsigned char* h_stage = nullptr;
@@ -26,6 +27,19 @@ struct fq_ctx {
     std::vector<double> g_key;
     int g_n = -1;
     long long launches = 0;
+    // Optional per-kernel timing (fq_ctx_set_profiling): an event pair per
+    // launch, resolved when the profile is read.
+    struct ProfRec {
+        cudaEvent_t a, b;
+        int kind;
+        double bytes;
+    };
+    bool profiling = false;
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    double prof_ms[FQ_KIND_COUNT] = {};
+    double prof_bytes[FQ_KIND_COUNT] = {};
+    long long prof_count[FQ_KIND_COUNT] = {};
 };
 
 namespace fq {
@@ -47,5 +61,14 @@ int upload_graph(fq_ctx* ctx, const GraphPrep& g, const double* upper);
 // Waits until the pinned staging buffer can be rewritten.
 int stage_acquire(fq_ctx* ctx);
 int validate_ctx(fq_ctx* ctx);
+// After a stream sync: FQ_ERR_TIMEOUT (and clears the flag) if a kernel
+// recorded a bounded wait that gave up.
+int check_device_error(fq_ctx* ctx);
+
+// Profiling brackets around one kernel launch: prof_begin records the start
+// event (returns a token, -1 when profiling is off), prof_end the stop event
+// with the launch's kind and algorithmic HBM bytes.
+int prof_begin(fq_ctx* ctx);
+void prof_end(fq_ctx* ctx, int token, int kind, double bytes);
 
 }  // namespace fq

@@ -7,8 +7,11 @@
 #include <algorithm>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "fq_ctx.h"
 #include "fq_pass.cuh"
+#include "fq_pass_tma.cuh"
 
 namespace fq {
 
@@ -129,21 +132,160 @@ __global__ void k_cut_small(const double2* sv, int N, const double* w, double* e
 
 // ------------------------------------------------------------ pass launch --
 
-template <typename WT, int PH, int GM, int EX, bool ST>
+// Kind of a pass for profiling, and the HBM bytes it must move.
+template <int PH, int GM, int EX, bool ST>
+static int pass_kind() {
+    if (EX == EX_ENERGY && !ST) return FQ_KIND_EXPECT;
+    if (EX == EX_DIAG) return FQ_KIND_EXPECT;
+    if (GM == GM_FULL) return FQ_KIND_RX;
+    if (GM == GM_NONE) return FQ_KIND_COST;
+    return PH != PH_NONE ? FQ_KIND_LAYER_PASS : FQ_KIND_STRIDED_PASS;
+}
+
+template <int PH, int EX, bool ST>
+static double pass_bytes(int N) {
+    const double n = (double)(1ull << N);
+    const bool load = (PH != PH_INIT) && (ST || EX == EX_ENERGY);
+    return n * ((load ? 16.0 : 0.0) + (ST ? 16.0 : 0.0) + (EX == EX_DIAG ? 8.0 : 0.0));
+}
+
+template <typename WT, int PH, int GM, int EX, bool ST, int SC>
 static int launch_pass(fq_ctx* ctx, const PassArgs& A) {
-    auto fn = k_pass<WT, PH, GM, EX, ST>;
+    auto fn = k_pass<WT, PH, GM, EX, ST, SC>;
     const size_t smem = pass_smem_bytes<WT>(A.N);
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pass_smem_bytes<WT>(kMaxQubits)));
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
+    const int tok = prof_begin(ctx);
     fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A);
     FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, pass_kind<PH, GM, EX, ST>(), pass_bytes<PH, EX, ST>(A.N));
     ctx->launches++;
     return FQ_OK;
 }
 
+// ------------------------------------------------------------ TMA pass --
+
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Whether TMA passes are used (FQ_TMA=0 selects the per-thread-load pass).
+static bool tma_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("FQ_TMA");
+        on = e ? (atoi(e) != 0) : 1;
+    }
+    return on != 0;
+}
+
+// The state as a tensor of float64 whose innermost dimension is one 128-byte
+// row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
+// Returns false for tiles with rows narrower than 8 amplitudes.
+static bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G) {
+    auto enc = tmap_encoder();
+    if (!enc || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
+    const int N = A.N, l = A.l, a = A.a, k = kTileBits - l;
+    cuuint64_t dims[5];
+    cuuint64_t strides[4];
+    cuuint32_t box[5];
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    int rank;
+    if (l == kTileBits) {
+        rank = 3;
+        G->kind = TG_CONTIG;
+        dims[0] = 16; dims[1] = 256; dims[2] = 1ull << (N - 11);
+        strides[0] = 128; strides[1] = 128ull * 256;
+        box[0] = 16; box[1] = 256; box[2] = 2;
+    } else if (l >= 4 && l <= 11) {
+        rank = 5;
+        G->kind = TG_ROWS;
+        dims[0] = 16; dims[1] = 1ull << (l - 3); dims[2] = 1ull << (a - l);
+        dims[3] = 1ull << k; dims[4] = 1ull << (N - a - k);
+        strides[0] = 128; strides[1] = 16ull << l; strides[2] = 16ull << a;
+        strides[3] = 16ull << (a + k);
+        box[0] = 16; box[1] = 1u << (l - 3); box[2] = 1; box[3] = 1u << k; box[4] = 1;
+    } else if (l == 3) {
+        rank = 5;
+        G->kind = TG_ROWS8;
+        dims[0] = 16; dims[1] = 1ull << (a - 3); dims[2] = 32; dims[3] = 16;
+        dims[4] = 1ull << (N - a - 9);
+        strides[0] = 128; strides[1] = 16ull << a; strides[2] = 16ull << (a + 5);
+        strides[3] = 16ull << (a + 9);
+        box[0] = 16; box[1] = 1; box[2] = 32; box[3] = 16; box[4] = 1;
+    } else {
+        return false;
+    }
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, (void*)A.sv, dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <typename WT, int PH, int GM, int EX, int SC>
+static int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, TmaGeom G) {
+    auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
+    const size_t smem = tma_pass_smem_bytes<WT>(A.N);
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
+    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
+    const int tok = prof_begin(ctx);
+    fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A, map, G);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
+    ctx->launches++;
+    return FQ_OK;
+}
+
+// Passes without RX (cost phase, <C>, cut diagonal) use the L0 schedule.
+// Passes that read and write the state run as TMA pipelines where the tile
+// geometry allows; write-only (layer-0) and read-only passes use k_pass.
+template <typename WT, int PH, int GM, int EX, bool ST>
+static int launch_pass(fq_ctx* ctx, const PassArgs& A) {
+    if (GM == GM_NONE && !(ST && PH == PH_MUL)) return launch_pass<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
+    const int sc = GM == GM_NONE ? SC_L0 : schedule_for(A.tmask);
+    if (ST && PH != PH_INIT && EX != EX_DIAG && tma_enabled()) {
+        alignas(64) CUtensorMap map;
+        TmaGeom G;
+        if (make_pass_tmap(A, &map, &G)) {
+            constexpr int EXT = EX == EX_ENERGY ? EX_ENERGY : EX_NONE;
+            switch (sc) {
+                case SC_L021: return launch_tma<WT, PH, GM, EXT, SC_L021>(ctx, A, map, G);
+                case SC_L01: return launch_tma<WT, PH, GM, EXT, SC_L01>(ctx, A, map, G);
+                default: return launch_tma<WT, PH, GM, EXT, SC_L0>(ctx, A, map, G);
+            }
+        }
+    }
+    switch (sc) {
+        case SC_L021: return launch_pass<WT, PH, GM, EX, ST, SC_L021>(ctx, A);
+        case SC_L01: return launch_pass<WT, PH, GM, EX, ST, SC_L01>(ctx, A);
+        default: return launch_pass<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
+    }
+}
+
 static int pass_grid(fq_ctx* ctx, const PassArgs& A) {
     return (int)std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
+}
+
+// Whether launch_pass will run A as a TMA pipeline (one CTA per SM).
+static bool runs_as_tma(const PassArgs& A, int ph) {
+    if (!tma_enabled() || ph == PH_INIT) return false;
+    if (!tmap_encoder() || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
+    return A.l >= 3;
 }
 
 template <typename WT, int PH, int EX>
@@ -221,6 +363,16 @@ static void gate_params(double beta, int& gm, double& g, double& f) {
     }
 }
 
+// Tiles a pass prefetches ahead into L2 (FQ_PREFETCH overrides, 0 = off).
+static int prefetch_distance() {
+    static int d = -1;
+    if (d < 0) {
+        const char* e = getenv("FQ_PREFETCH");
+        d = e ? std::max(0, std::min(4, atoi(e))) : 1;
+    }
+    return d;
+}
+
 static PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     PassArgs A;
     memset(&A, 0, sizeof(A));
@@ -238,6 +390,8 @@ static PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     A.ntab = g.integer ? (int)(g.cmax - g.cmin + 1) : 1;
     A.W = g.integer ? (double)g.W_int : g.W;
     A.scale = 1.0;
+    A.pf_dist = prefetch_distance();
+    A.err = ctx->d_err;
     return A;
 }
 
@@ -254,6 +408,7 @@ static int read_result(fq_ctx* ctx, double* host) {
     FQ_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, sizeof(double), cudaMemcpyDeviceToHost,
                             ctx->stream));
     FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    FQ_TRY(check_device_error(ctx));
     *host = ctx->h_result[0];
     return FQ_OK;
 }
@@ -341,7 +496,8 @@ int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph,
                 FQ_TRY(launch_engine_pass<int>(ctx, ph, gm, ex, A));
             else
                 FQ_TRY(launch_engine_pass<double>(ctx, ph, gm, ex, A));
-            last_grid = pass_grid(ctx, A);
+            last_grid = runs_as_tma(A, ph) ? (int)std::min<i64>(A.ntiles, ctx->num_sms)
+                                           : pass_grid(ctx, A);
         }
     }
     if (energy) {

@@ -19,9 +19,15 @@
 // Three layouts rotate which 4 tile bits are register bits; moving between
 // them goes through a 64 KB shared buffer with an XOR swizzle that keeps
 // every quarter-warp's 16-byte accesses in distinct banks:
-//   L0 (load/store): regs = tile bits 8..11, lanes = 0..4,  warps = 5..7
-//   L1:              regs = tile bits 4..7,  lanes = 0..3,8, warps = 9..11
+//   L0 (load):       regs = tile bits 8..11, lanes = 0..4,  warps = 5..7
+//   L1 (store):      regs = tile bits 4..7,  lanes = 0..3,8, warps = 9..11
 //   L2:              regs = tile bits 0..3,  lanes = 4..8,  warps = 9..11
+// L0 and L1 both keep the row bits on consecutive lanes, so a tile is loaded
+// in L0 and stored from L1 without a layout change of its own: 12 qubits
+// take two exchanges (L0 -> L2 -> L1), 8 take one (L0 -> L1).  A single
+// qubit among tile bits 0..3 is rotated with warp shuffles instead (those
+// bits are lane bits in L0 and L1), so a strided pass with 128-byte rows
+// (9 qubits, tile bits 3..11) also needs one exchange.
 //
 // Cut value of an amplitude (exact in integers for integer weights):
 //   C(z) = K(fixed) + C_TT(tile bits) + sum_{u in tile} z_u e_u(fixed)
@@ -46,6 +52,16 @@ constexpr int kMaxFixed = kMaxQubits - kTileBits;  // 21
 enum { PH_NONE = 0, PH_MUL = 1, PH_INIT = 2 };
 // Extra outputs: none, <C> partial sums, cut value of every amplitude
 enum { EX_NONE = 0, EX_ENERGY = 1, EX_DIAG = 2 };
+// Round schedules: L0 only; L0 -> L1; L0 -> L2 -> L1 (see header comment).
+enum { SC_L0 = 0, SC_L01 = 1, SC_L021 = 2 };
+
+// Schedule a target mask needs.
+__host__ __device__ inline int schedule_for(unsigned tmask) {
+    const unsigned lo = tmask & 15u, mid = (tmask >> 4) & 15u;
+    if (lo & (lo - 1)) return SC_L021;  // two or more of tile bits 0..3
+    if (mid) return SC_L01;
+    return SC_L0;
+}
 // Gate modes: reduced RX [[1,-it],[-it,1]] (t = tan(b/2)), reduced RX
 // [[u,-i],[-i,u]] (u = cot(b/2)), the full RX of src/rx.cu:47-50.
 enum { GM_NONE = 0, GM_TAN = 1, GM_COT = 2, GM_FULL = 3 };
@@ -65,6 +81,8 @@ struct PassArgs {
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
     double W;        // total weight
     double scale;    // multiplies the phase
+    int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
+    int* err;        // device error flag (bounded waits that gave up)
 };
 
 __device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j : a + j - l; }
@@ -107,6 +125,31 @@ __device__ __forceinline__ void rx_regs(double2 (&v)[kRegs], unsigned m4, double
     }
 }
 
+// RX on a qubit held in lane bit j: every lane updates its own amplitude
+// from its partner's (the gate is symmetric in the pair: self' = a*self -
+// i*b*partner).
+template <int GM>
+__device__ __forceinline__ void rx_lane(double2 (&v)[kRegs], int j, double g, double c, double s) {
+    const unsigned lm = 1u << j;
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) {
+        double2 q;
+        q.x = __shfl_xor_sync(0xffffffffu, v[r].x, lm);
+        q.y = __shfl_xor_sync(0xffffffffu, v[r].y, lm);
+        const double2 m = v[r];
+        if (GM == GM_TAN) {
+            v[r].x = fma(g, q.y, m.x);
+            v[r].y = fma(-g, q.x, m.y);
+        } else if (GM == GM_COT) {
+            v[r].x = fma(g, m.x, q.y);
+            v[r].y = fma(g, m.y, -q.x);
+        } else {
+            v[r].x = m.x * c + q.y * s;
+            v[r].y = m.y * c - q.x * s;
+        }
+    }
+}
+
 // Tile index held in register r under layout L (see header comment).
 template <int L>
 __device__ __forceinline__ int lay_index(int tid, int r) {
@@ -129,18 +172,19 @@ __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int 
 // Shared-memory bytes a pass needs for N qubits and weight type WT.
 template <typename WT>
 __host__ __device__ inline size_t pass_smem_bytes(int N) {
-    return sizeof(double2) * kTile + sizeof(double) * 8 + sizeof(int) * 24 +
+    return sizeof(double2) * kTile + sizeof(double) * 8 + sizeof(i64) * 32 + sizeof(int) * 24 +
            sizeof(WT) * (N * N + 32 + 16 + 24 + 16);
 }
 
-template <typename WT, int PH, int GM, int EX, bool ST>
+template <typename WT, int PH, int GM, int EX, bool ST, int SC>
 __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2* buf = reinterpret_cast<double2*>(smraw);
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
     double* red = reinterpret_cast<double*>(buf + kTile);  // 8 warp partials
-    int* fpos = reinterpret_cast<int*>(red + 8);           // nF fixed positions, ascending
+    i64* offtab = reinterpret_cast<i64*>(red + 8);          // register-slot offsets: L0, L1
+    int* fpos = reinterpret_cast<int*>(offtab + 32);        // nF fixed positions, ascending
     WT* sw = reinterpret_cast<WT*>(fpos + 24);             // N*N weights
     WT* ke = sw + N * N;                                   // [0] = K, [1+u] = e_u
     WT* creg = ke + 32;                                    // 16: cut among register bits
@@ -151,6 +195,14 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
 
+    if (tid < 2 * kRegs) {
+        // Offset of register slot r: tile bits 8..11 in L0, 4..7 in L1.
+        const int r = tid & 15, lo = tid < kRegs ? 8 : 4;
+        i64 o = 0;
+        for (int k = 0; k < 4; k++)
+            if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
+        offtab[tid] = o;
+    }
     if (CUT) {
         const WT* gw = reinterpret_cast<const WT*>(A.w);
         for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
@@ -204,17 +256,44 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         }
     }
     // Address pieces: thread part and the 4 register-bit strides (layout L0).
-    i64 thr_off = 0;
+    i64 thr_off = 0, thr_off1 = 0;
     for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    const i64 rb0 = 1ll << tile_phys(8, l, a), rb1 = 1ll << tile_phys(9, l, a);
-    const i64 rb2 = 1ll << tile_phys(10, l, a), rb3 = 1ll << tile_phys(11, l, a);
+    {
+        const int t1 = lay_index<1>(tid, 0);
+        for (int j = 0; j < kTileBits; j++)
+            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
+    }
+    const int pf_step = l < 3 ? l : 3;  // prefetch granularity: 128-byte lines or rows
+    const bool contiguous = (l == kTileBits);
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
-    const bool need_l1 = (m_mid | m_lo) != 0;
-    const bool need_l2 = m_lo != 0;
+    // Tile bits 0..3: two or more targets take a register round in L2
+    // (SC_L021), a single one is rotated by shuffles in L0.
+    const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double acc = 0, comp = 0;  // Kahan-compensated <C> accumulator
 
     for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x) {
         const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        if (LOAD && A.pf_dist > 0) {
+            // Stream this CTA's tile pf_dist strides ahead from HBM into L2
+            // while the current one is computed: the loads below then hit L2.
+            const i64 T2 = T + (i64)A.pf_dist * gridDim.x;
+            if (T2 < A.ntiles) {
+                const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
+                               ((T2 >> nmid) << (a + kTileBits - l));
+                if (contiguous) {
+                    if (tid == 0)
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
+                                     "r"((unsigned)(kTile * sizeof(double2)))
+                                     : "memory");
+                } else {
+                    for (int j = tid; j < (1 << (kTileBits - pf_step)); j += kPassThreads) {
+                        const int t = j << pf_step;
+                        const i64 off = (i64)(t & ((1 << l) - 1)) | ((i64)(t >> l) << a);
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + b2 + off) : "memory");
+                    }
+                }
+            }
+        }
         if (CUT) {
             __syncthreads();  // previous tile's readers of ke are done
             if (warp == 0) {
@@ -255,9 +334,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         }
 #pragma unroll
         for (int r = 0; r < kRegs; r++) {
-            const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
-                            ((r & 8) ? rb3 : 0);
-            if (LOAD) v[r] = __ldcs(p + off);
+            if (LOAD) v[r] = __ldcs(p + offtab[r]);
             else v[r] = make_double2(0.0, 0.0);
         }
         if (PH != PH_NONE) {
@@ -292,18 +369,22 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 }
             }
         }
+        // Final layout: L1 after an exchange, L0 for <C> (the cut
+        // decomposition is per L0 slot).
+        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE) ? 1 : 0;
         if (GM != GM_NONE) {
             rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
-            if (need_l1) {
+            if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
+            if (SC == SC_L021) {
+                exchange<0, 2>(v, buf, tid);
+                rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
+                exchange<2, 1>(v, buf, tid);
+            } else if (SC == SC_L01) {
                 exchange<0, 1>(v, buf, tid);
+            }
+            if (SC != SC_L0) {
                 rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                if (need_l2) {
-                    exchange<1, 2>(v, buf, tid);
-                    rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
-                    exchange<2, 0>(v, buf, tid);
-                } else {
-                    exchange<1, 0>(v, buf, tid);
-                }
+                if (LAY == 0) exchange<1, 0>(v, buf, tid);
             }
         }
         if (EX == EX_DIAG) {
@@ -311,9 +392,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             for (int r = 0; r < kRegs; r++) {
                 const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
-                const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
-                                ((r & 8) ? rb3 : 0);
-                __stcs(A.diag + base + thr_off + off, (double)cr);
+                __stcs(A.diag + base + thr_off + offtab[r], (double)cr);
             }
         }
         if (EX == EX_ENERGY) {
@@ -330,11 +409,13 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             acc = t2;
         }
         if (ST) {
+            if (LAY == 0) {
 #pragma unroll
-            for (int r = 0; r < kRegs; r++) {
-                const i64 off = ((r & 1) ? rb0 : 0) + ((r & 2) ? rb1 : 0) + ((r & 4) ? rb2 : 0) +
-                                ((r & 8) ? rb3 : 0);
-                __stcs(p + off, v[r]);
+                for (int r = 0; r < kRegs; r++) __stcs(p + offtab[r], v[r]);
+            } else {
+                double2* const p1 = A.sv + base + thr_off1;
+#pragma unroll
+                for (int r = 0; r < kRegs; r++) __stcs(p1 + offtab[kRegs + r], v[r]);
             }
         }
     }

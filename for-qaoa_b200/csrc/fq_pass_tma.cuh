@@ -1,0 +1,365 @@
+// fq_pass_tma.cuh -- the streaming tile pass as a persistent TMA pipeline.
+//
+// Same tile, thread layouts, cut decomposition and RX rounds as k_pass
+// (fq_pass.cuh), but tiles reach shared memory through the Tensor Memory
+// Accelerator instead of per-thread loads, so HBM keeps streaming while the
+// CTA computes:
+//   - one CTA per SM loops over its tiles; a ring of three 64 KB stage
+//     buffers holds the tile being computed and the next two in flight;
+//   - thread 0 issues one cp.async.bulk.tensor copy per tile (a 3-D or 5-D
+//     box over the state seen as rows of 8 amplitudes = 128 bytes, 128-byte
+//     swizzle, no multicast), completion counted on a per-stage mbarrier;
+//   - the 256 threads read the landed tile into registers (layout L0),
+//     rotate, exchange through the same buffer, and store with 16-byte
+//     streaming stores straight from registers (layout L1), so no second
+//     copy of the tile is staged for the way out.
+// Every mbarrier wait is bounded: on expiry the CTA records an error flag
+// the host reports as FQ_ERR_TIMEOUT, drains the copies it issued (again
+// bounded) and returns.
+#pragma once
+
+#include <cuda.h>
+
+#include "fq_pass.cuh"
+
+namespace fq {
+
+constexpr int kStages = 3;
+constexpr unsigned kTileBytes = kTile * sizeof(double2);  // 64 KB
+constexpr long long kWaitSpins = 1ll << 22;              // bound on mbarrier polls
+
+// Box geometry of a pass (host-chosen, see make_pass_tmap):
+//   TG_CONTIG  l = 12: rank 3, box {16 doubles, 256 rows, 2}
+//   TG_ROWS    4 <= l <= 11: rank 5, box {16, 2^(l-3), 1, 2^(12-l), 1}
+//   TG_ROWS8   l = 3: rank 5, box {16, 1, 32, 16, 1}
+enum { TG_CONTIG = 0, TG_ROWS = 1, TG_ROWS8 = 2 };
+
+struct TmaGeom {
+    int kind;
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of an mbarrier; false if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (long long i = 0; i < kWaitSpins; i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map,
+                                            unsigned long long* bar, int c0, int c1, int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_addr(dst)),
+        "l"((unsigned long long)map), "r"(smem_addr(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map,
+                                            unsigned long long* bar, int c0, int c1, int c2,
+                                            int c3, int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_addr(dst)),
+        "l"((unsigned long long)map), "r"(smem_addr(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "r"(c4)
+        : "memory");
+}
+
+// Slot of tile index t in a buffer written by TMA with the 128-byte swizzle:
+// 16-byte chunk bits 0..2 are XORed with the 128-byte row bits 0..2.
+__device__ __forceinline__ int tslot(int t) { return t ^ ((t >> 3) & 7); }
+
+// Shared-memory bytes of the TMA pass (1 KB of alignment slack included).
+template <typename WT>
+__host__ __device__ inline size_t tma_pass_smem_bytes(int N) {
+    return 1024 + (size_t)kStages * kTileBytes + 64 + sizeof(double) * 8 + sizeof(i64) * 32 +
+           sizeof(int) * 24 + sizeof(WT) * (N * N + 32 + 16 + 24 + 16);
+}
+
+template <typename WT, int PH, int GM, int EX, int SC>
+__global__ void __launch_bounds__(kPassThreads, 1)
+    k_pass_tma(const PassArgs A, const __grid_constant__ CUtensorMap tmap, const TmaGeom G) {
+    extern __shared__ unsigned char smraw[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~(uintptr_t)1023);
+    double2* stage = reinterpret_cast<double2*>(sm);
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + kStages * kTileBytes);
+    int* s_abort = reinterpret_cast<int*>(full + kStages);
+    double* red = reinterpret_cast<double*>(full + 8);
+    i64* offtab = reinterpret_cast<i64*>(red + 8);
+    int* fpos = reinterpret_cast<int*>(offtab + 32);
+    WT* sw = reinterpret_cast<WT*>(fpos + 24);
+    WT* ke = sw + A.N * A.N;
+    WT* creg = ke + 32;
+    WT* Dm = creg + 16;
+    WT* Ru = Dm + 24;
+    constexpr bool CUT = (PH != PH_NONE) || (EX == EX_ENERGY);
+    const int N = A.N, l = A.l, a = A.a;
+    const int nF = N - kTileBits;
+    const int nmid = a - l;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const i64 my_tiles =
+        blockIdx.x < A.ntiles ? (A.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    // Issue the copy of this CTA's tile j into stage j % kStages.
+    auto issue = [&](i64 j) {
+        const i64 T = blockIdx.x + j * (i64)gridDim.x;
+        const int s = (int)(j % kStages);
+        void* dst = stage + (size_t)s * kTile;
+        mbar_expect_tx(&full[s], kTileBytes);
+        if (G.kind == TG_CONTIG) {
+            tma_load_3d(dst, &tmap, &full[s], 0, 0, (int)(2 * T));
+        } else if (G.kind == TG_ROWS) {
+            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)(T & ((1ll << nmid) - 1)), 0,
+                        (int)(T >> nmid));
+        } else {
+            tma_load_5d(dst, &tmap, &full[s], 0, (int)(T & ((1ll << nmid) - 1)), 0, 0,
+                        (int)(T >> nmid));
+        }
+    };
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; s++) mbar_init(&full[s], 1);
+        *s_abort = 0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (tid < 2 * kRegs) {
+        const int r = tid & 15, lo = tid < kRegs ? 8 : 4;
+        i64 o = 0;
+        for (int k = 0; k < 4; k++)
+            if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
+        offtab[tid] = o;
+    }
+    if (CUT) {
+        const WT* gw = reinterpret_cast<const WT*>(A.w);
+        for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
+        if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (i64 j = 0; j < kStages - 1 && j < my_tiles; j++) issue(j);
+    if (CUT) {
+        if (tid < nF) {
+            const int m = fpos[tid];
+            WT d = 0;
+            for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
+            Dm[tid] = d;
+        } else if (tid >= 32 && tid < 32 + kTileBits) {
+            const int u = tile_phys(tid - 32, l, a);
+            WT r = 0;
+            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
+            Ru[tid - 32] = r;
+        } else if (tid >= 64 && tid < 80) {
+            const int r = tid - 64;
+            WT c = 0;
+            for (int k = 0; k < 4; k++)
+                for (int k2 = k + 1; k2 < 4; k2++)
+                    if (((r >> k) ^ (r >> k2)) & 1)
+                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
+            creg[r] = c;
+        }
+    }
+    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
+    if (CUT) {
+        for (int j = 0; j < 8; j++) {
+            const int pj = tile_phys(j, l, a);
+            const int tj = (tid >> j) & 1;
+            for (int j2 = j + 1; j2 < 8; j2++)
+                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
+            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
+            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
+            if (tj) {
+                athr += w0 + w1 + w2 + w3;
+                f0 -= w0;
+                f1 -= w1;
+                f2 -= w2;
+                f3 -= w3;
+            } else {
+                f0 += w0;
+                f1 += w1;
+                f2 += w2;
+                f3 += w3;
+            }
+        }
+    }
+    i64 thr_off = 0, thr_off1 = 0;
+    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
+    {
+        const int t1 = lay_index<1>(tid, 0);
+        for (int j = 0; j < kTileBits; j++)
+            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
+    }
+    const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
+    const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
+    double acc = 0, comp = 0;
+    i64 j = 0;
+
+    for (; j < my_tiles; j++) {
+        const i64 T = blockIdx.x + j * (i64)gridDim.x;
+        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        const int s = (int)(j % kStages);
+        double2* buf = stage + (size_t)s * kTile;
+        __syncthreads();  // tile j-1 is finished: its stage may be refilled
+        if (tid == 0 && j + kStages - 1 < my_tiles) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(j + kStages - 1);
+        }
+        if (CUT && warp == 0) {
+            WT h = 0;
+            if (lane < nF) {
+                const int m = fpos[lane];
+                const int zm = (int)((base >> m) & 1);
+                if (zm) h += Dm[lane];
+                for (int i = lane + 1; i < nF; i++)
+                    if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+            if (lane < kTileBits) {
+                const int u = tile_phys(lane, l, a);
+                WT e = Ru[lane];
+                for (int i = 0; i < nF; i++)
+                    if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
+                ke[1 + lane] = e;
+            }
+            if (lane == 0) ke[0] = h;
+        }
+        if (!mbar_wait_bounded(&full[s], (unsigned)((j / kStages) & 1))) {
+            *s_abort = 1;
+            if (A.err) atomicExch(A.err, 1);
+        }
+        __syncthreads();  // tile landed (or abort), ke visible
+        if (*s_abort) break;
+
+        double2 v[kRegs];
+#pragma unroll
+        for (int r = 0; r < kRegs; r++) v[r] = buf[tslot(lay_index<0>(tid, r))];
+        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+        if (CUT) {
+            cbase = ke[0] + athr;
+#pragma unroll
+            for (int jj = 0; jj < 8; jj++)
+                if ((tid >> jj) & 1) cbase += ke[1 + jj];
+            g0 = f0 + ke[9];
+            g1 = f1 + ke[10];
+            g2 = f2 + ke[11];
+            g3 = f3 + ke[12];
+        }
+        if (PH != PH_NONE) {
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                double2 ph;
+                if (sizeof(WT) == sizeof(int)) {
+                    const int ti = min(max((int)cr - A.cmin, 0), A.ntab - 1);
+                    ph = __ldg(A.ptab + ti);
+                } else {
+                    const double S = 2.0 * (double)cr - A.W;
+                    double sn, cs;
+                    sincos(S * A.gamma / 2, &sn, &cs);
+                    ph.x = cs;
+                    ph.y = sn;
+                }
+                if (PH == PH_INIT) {
+                    v[r].x = ph.x * A.scale;
+                    v[r].y = ph.y * A.scale;
+                } else {
+                    if (sizeof(WT) != sizeof(int)) {
+                        ph.x *= A.scale;
+                        ph.y *= A.scale;
+                    }
+                    const double2 in = v[r];
+                    v[r].x = in.x * ph.x - in.y * ph.y;
+                    v[r].y = in.x * ph.y + in.y * ph.x;
+                }
+            }
+        }
+        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE) ? 1 : 0;
+        if (GM != GM_NONE) {
+            rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
+            if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
+            if (SC == SC_L021) {
+                exchange<0, 2>(v, buf, tid);
+                rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
+                exchange<2, 1>(v, buf, tid);
+            } else if (SC == SC_L01) {
+                exchange<0, 1>(v, buf, tid);
+            }
+            if (SC != SC_L0) {
+                rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
+                if (LAY == 0) exchange<1, 0>(v, buf, tid);
+            }
+        }
+        if (EX == EX_ENERGY) {
+            double ts = 0;
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
+            }
+            const double y = ts - comp;
+            const double t2 = acc + y;
+            comp = (t2 - acc) - y;
+            acc = t2;
+        }
+        if (LAY == 0) {
+            double2* const p = A.sv + base + thr_off;
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) __stcs(p + offtab[r], v[r]);
+        } else {
+            double2* const p1 = A.sv + base + thr_off1;
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) __stcs(p1 + offtab[kRegs + r], v[r]);
+        }
+    }
+    if (*s_abort) {
+        // Drain the copies still in flight into this CTA's stages (bounded).
+        if (tid == 0)
+            for (i64 k = j; k < j + kStages && k < my_tiles; k++)
+                mbar_wait_bounded(&full[k % kStages], (unsigned)((k / kStages) & 1));
+        return;
+    }
+    if (EX == EX_ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        __syncthreads();
+        if (lane == 0) red[warp] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double sum = 0;
+            for (int w = 0; w < kPassThreads / 32; w++) sum += red[w];
+            A.partial[blockIdx.x] = sum;
+        }
+    }
+}
+
+}  // namespace fq

@@ -104,8 +104,11 @@ extern "C" int fq_swap_blocks(fq_ctx* ctx, void* sv, int N, int swap_out, int sw
     S.nitems = S.npairs << S.nob;
     const size_t smem = sizeof(double2) * 2 * (1 << S.a) * ((1 << (S.a + S.eb)) + 1);
     const i64 grid = std::min<i64>(S.nitems, (i64)ctx->num_sms * 8);
+    const int tok = prof_begin(ctx);
     k_swap_blocks<<<(unsigned)grid, 256, smem, ctx->stream>>>(S);
     FQ_CUDA(cudaGetLastError());
+    // Amplitudes whose two blocks hold equal values stay put.
+    prof_end(ctx, tok, FQ_KIND_SWAP, 32.0 * (double)(1ull << N) * (1.0 - 1.0 / (1ull << num_swap)));
     ctx->launches++;
     return FQ_OK;
 }

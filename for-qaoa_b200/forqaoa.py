@@ -17,6 +17,10 @@ LIB_PATH = os.path.join(HERE, "libforqaoa.so")
 
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BUSY = range(7)
 
+# Kernel kinds of fq_ctx_profile (include/forqaoa.h)
+KINDS = {"layer_pass": 0, "strided_pass": 1, "cost": 2, "rx": 3, "swap": 4, "expect": 5,
+         "other": 6}
+
 if not os.path.exists(LIB_PATH):
     raise ImportError("libforqaoa.so not built: run `make -C for-qaoa_b200` "
                       "(or __graft_entry__.build())")
@@ -39,6 +43,9 @@ SIGNATURES = {
     "fq_ctx_stream": (_vp, [_vp]),
     "fq_ctx_kernel_launches": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "fq_ctx_device_info": (_i, [_vp, _ip, _ip]),
+    "fq_ctx_set_profiling": (_i, [_vp, _i]),
+    "fq_ctx_profile": (_i, [_vp, _i, _dp, ctypes.POINTER(ctypes.c_longlong), _dp]),
+    "fq_ctx_profile_reset": (_i, [_vp]),
     "fq_state_alloc": (_i, [_vp, _i, ctypes.POINTER(_vp)]),
     "fq_state_free": (_i, [_vp, _vp]),
     "fq_state_init_basis0": (_i, [_vp, _vp, _i]),
@@ -180,6 +187,23 @@ class Context:
         _check(_lib.fq_ctx_kernel_launches(self.handle, ctypes.byref(c)),
                "fq_ctx_kernel_launches")
         return c.value
+
+    def set_profiling(self, on=True):
+        _check(_lib.fq_ctx_set_profiling(self.handle, int(bool(on))), "fq_ctx_set_profiling")
+
+    def profile_reset(self):
+        _check(_lib.fq_ctx_profile_reset(self.handle), "fq_ctx_profile_reset")
+
+    def profile(self):
+        """{kind: (device ms, launches, algorithmic bytes)} since the last reset."""
+        out = {}
+        for name, k in KINDS.items():
+            ms, n, b = _d(), ctypes.c_longlong(), _d()
+            _check(_lib.fq_ctx_profile(self.handle, k, ctypes.byref(ms), ctypes.byref(n),
+                                       ctypes.byref(b)), "fq_ctx_profile")
+            if n.value:
+                out[name] = (ms.value, n.value, b.value)
+        return out
 
     def device_info(self):
         a, b = _i(), _i()

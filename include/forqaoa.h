@@ -60,6 +60,25 @@ int fq_ctx_kernel_launches(fq_ctx* ctx, long long* count);
 /* Resident CTAs per SM and SM count the streaming kernels are sized for. */
 int fq_ctx_device_info(fq_ctx* ctx, int* num_sms, int* ctas_per_sm);
 
+/* Per-kernel timing.  While enabled, every library kernel launch is
+ * bracketed by CUDA events on the context's stream; fq_ctx_profile
+ * synchronises the stream and returns, for one kernel kind, the summed
+ * device time (ms), the launch count and the summed algorithmic HBM bytes
+ * (bytes the kernel must move: 16 per amplitude read, 16 per amplitude
+ * written).  Kinds: */
+#define FQ_KIND_LAYER_PASS 0    /* fused pass: cost phase + RX on 12 low qubits */
+#define FQ_KIND_STRIDED_PASS 1  /* fused pass: RX on high qubits, strided tile */
+#define FQ_KIND_COST 2          /* fq_cost_phase */
+#define FQ_KIND_RX 3            /* fq_rx_chunk / fq_rx_targets */
+#define FQ_KIND_SWAP 4          /* fq_swap_blocks */
+#define FQ_KIND_EXPECT 5        /* <C> / cut diagonal sweeps */
+#define FQ_KIND_OTHER 6         /* tables, reductions, permutations */
+#define FQ_KIND_COUNT 8
+int fq_ctx_set_profiling(fq_ctx* ctx, int enable);
+int fq_ctx_profile(fq_ctx* ctx, int kind, double* total_ms, long long* launches,
+                   double* bytes);
+int fq_ctx_profile_reset(fq_ctx* ctx);
+
 /* ---- state memory (include/state.h, src/state.cpp) ---------------------- */
 /* cudaMalloc of 16 * 2^N bytes; replaces createState's allocation
  * (src/state.cpp:89-159, D = 0). */

@@ -331,6 +331,28 @@ void orc_energy_grad(int N, int P, const double* graph_upper, const double* gamm
     free(lam);
 }
 
+void orc_layer_sample(double* sv, int N, int s, const double* graph1d, double gamma,
+                      double beta, double* t_cost, double* t_rx) {
+    const i64 n = 1ll << s;
+    const double amp = orc_init_amp(N);
+    double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(static)
+    for (i64 b = 0; b < n; b++) {
+        double sum = pair_sum((u64)b, N, graph1d);
+        double sn, cs;
+        sincos(sum * gamma / 2, &sn, &cs);
+        sv[2 * b] = cs * amp;
+        sv[2 * b + 1] = sn * amp;
+    }
+    double t1 = omp_get_wtime();
+    int targets[64];
+    for (int q = 0; q < s; q++) targets[q] = q;
+    orc_multi_rotate_x(sv, s, targets, s, beta);
+    double t2 = omp_get_wtime();
+    *t_cost = t1 - t0;
+    *t_rx = t2 - t1;
+}
+
 void orc_permute_qubits(const double* src, double* dst, int N, const int* perm) {
     const i64 n = 1ll << N;
 #pragma omp parallel for schedule(static)

@@ -66,6 +66,13 @@ void orc_energy_grad(int N, int P, const double* graph_upper, const double* gamm
                      double* grad_beta);
 /* dst[y] = src[x] where y has bit perm[b] equal to bit b of x. */
 void orc_permute_qubits(const double* src, double* dst, int N, const int* perm);
+/* CPU-baseline sample of one QAOA layer of an N-qubit circuit: the cost
+ * phase of rzz.cu:121-156 (pair loop over the full N-qubit graph) on the
+ * first 2^s amplitudes, then RX (rx.cu:32-53) on qubits 0..s-1 of that
+ * slice.  Returns the seconds each half took; a full layer is
+ * t_cost * 2^(N-s) + t_rx * (N * 2^(N-1)) / (s * 2^(s-1)). */
+void orc_layer_sample(double* sv, int N, int s, const double* graph1d, double gamma,
+                      double beta, double* t_cost, double* t_rx);
 /* Threads OpenMP will use. */
 int orc_num_threads(void);
 

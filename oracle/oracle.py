@@ -51,6 +51,8 @@ def lib():
                                       _dp, _dp, _dp]
         L.orc_permute_qubits.argtypes = [_dp, _dp, ctypes.c_int, _ip]
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_layer_sample.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double,
+                                       ctypes.c_double, _dp, _dp]
         _lib = L
     return _lib
 
@@ -187,3 +189,20 @@ def permute_qubits(sv, perm):
 def to_logical(sv_phys, label_map):
     """Physical-order state (reference layout) -> logical order."""
     return permute_qubits(sv_phys, label_map)
+
+
+def layer_sample(graph, s, gamma, beta):
+    """Time one layer's work units on a 2^s-amplitude slice of the N-qubit
+    circuit; returns (t_cost, t_rx, estimated seconds for the full layer)."""
+    g = _f64(graph)
+    n = g.shape[0]
+    g1d = upper_tri_to_1d(g)
+    if len(g1d) == 0:
+        g1d = np.zeros(1)
+    sv = np.zeros(1 << s, dtype=np.complex128)
+    tc = np.zeros(1)
+    tr = np.zeros(1)
+    lib().orc_layer_sample(sv.view(np.float64).ctypes.data_as(_dp), n, s, _d(g1d), gamma,
+                           beta, _d(tc), _d(tr))
+    full = tc[0] * 2.0 ** (n - s) + tr[0] * (n * 2.0 ** (n - 1)) / (s * 2.0 ** (s - 1))
+    return float(tc[0]), float(tr[0]), full
