@@ -31,6 +31,22 @@ __global__ void k_phase_table(double2* tab, int cmin, int n, long long W, double
     }
 }
 
+// Two-level phase table of the engine: tab[j] = exp(i*gamma*j) for j < 32,
+// tab[32 + h] = scale * (cos, sin)(S * gamma / 2) with S = 2(cmin + 32h) - W.
+__global__ void k_phase_table2(double2* tab, int cmin, int nhi, long long W, double gamma,
+                               double scale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double sn, cs;
+    if (i < kPhaseLo) {
+        sincos(gamma * (double)i, &sn, &cs);
+        tab[i] = make_double2(cs, sn);
+    } else if (i < kPhaseLo + nhi) {
+        const double S = (double)(2ll * (cmin + 32ll * (i - kPhaseLo)) - W);
+        sincos(S * gamma / 2, &sn, &cs);
+        tab[i] = make_double2(cs * scale, sn * scale);
+    }
+}
+
 // Deterministic sum of n partials into out[0]: fixed strided split and a
 // fixed tree, so the same inputs always give the same bits.
 __global__ void k_reduce_partials(const double* partial, int n, double* out) {
@@ -183,15 +199,26 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     return fn;
 }
 
-// Whether TMA passes are used (FQ_TMA=0 selects the per-thread-load pass).
-static bool tma_enabled() {
-    static int on = -1;
-    if (on < 0) {
+// Which passes run as TMA pipelines (FQ_TMA overrides; measured on B200 at
+// N=30, see the profiles):
+//   0  none (every pass uses per-thread loads, k_pass)
+//   1  passes without a cost phase use the one-group TMA pass (default:
+//      strided passes are fastest there, the phase pass with k_pass)
+//   2  every read-write pass uses the two-group TMA pass
+//   3  every read-write pass uses the one-group TMA pass
+static int tma_mode() {
+    static int m = -1;
+    if (m < 0) {
         const char* e = getenv("FQ_TMA");
-        on = e ? (atoi(e) != 0) : 1;
+        m = e ? std::max(0, std::min(3, atoi(e))) : 1;
     }
-    return on != 0;
+    return m;
 }
+static bool tma_for(int ph) {
+    const int m = tma_mode();
+    return m >= 2 || (m == 1 && ph == PH_NONE);
+}
+static int tma_groups() { return tma_mode() == 2 ? 2 : 1; }
 
 // The state as a tensor of float64 whose innermost dimension is one 128-byte
 // row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
@@ -238,13 +265,21 @@ static bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G) {
 
 template <typename WT, int PH, int GM, int EX, int SC>
 static int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, TmaGeom G) {
-    auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
-    const size_t smem = tma_pass_smem_bytes<WT>(A.N);
-    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
     const int tok = prof_begin(ctx);
-    fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A, map, G);
+    if (tma_groups() == 2) {
+        auto fn = k_pass_tma2<WT, PH, GM, EX, SC>;
+        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tma2_pass_smem_bytes<WT>(kMaxQubits)));
+        fn<<<(unsigned)grid, 2 * kPassThreads, tma2_pass_smem_bytes<WT>(A.N), ctx->stream>>>(
+            A, map, G);
+    } else {
+        auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
+        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
+        fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map,
+                                                                                        G);
+    }
     FQ_CUDA(cudaGetLastError());
     prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
     ctx->launches++;
@@ -258,7 +293,7 @@ template <typename WT, int PH, int GM, int EX, bool ST>
 static int launch_pass(fq_ctx* ctx, const PassArgs& A) {
     if (GM == GM_NONE && !(ST && PH == PH_MUL)) return launch_pass<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
     const int sc = GM == GM_NONE ? SC_L0 : schedule_for(A.tmask);
-    if (ST && PH != PH_INIT && EX != EX_DIAG && tma_enabled()) {
+    if (ST && PH != PH_INIT && EX != EX_DIAG && tma_for(PH)) {
         alignas(64) CUtensorMap map;
         TmaGeom G;
         if (make_pass_tmap(A, &map, &G)) {
@@ -283,7 +318,7 @@ static int pass_grid(fq_ctx* ctx, const PassArgs& A) {
 
 // Whether launch_pass will run A as a TMA pipeline (one CTA per SM).
 static bool runs_as_tma(const PassArgs& A, int ph) {
-    if (!tma_enabled() || ph == PH_INIT) return false;
+    if (!tma_for(ph) || ph == PH_INIT) return false;
     if (!tmap_encoder() || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
     return A.l >= 3;
 }
@@ -388,11 +423,33 @@ static PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     A.tmask = 0;
     A.cmin = (int)g.cmin;
     A.ntab = g.integer ? (int)(g.cmax - g.cmin + 1) : 1;
+    A.nhi = 0;
     A.W = g.integer ? (double)g.W_int : g.W;
     A.scale = 1.0;
     A.pf_dist = prefetch_distance();
     A.err = ctx->d_err;
     return A;
+}
+
+// High-part entries of the engine's two-level phase table (0: the range is
+// too wide for shared memory and the one-level global table is used).
+static int engine_nhi(const GraphPrep& g) {
+    const long long range = g.cmax - g.cmin + 1;
+    const long long nhi = (range + kPhaseLo - 1) / kPhaseLo;
+    return nhi <= kPhaseHiMax ? (int)nhi : 0;
+}
+
+static int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
+    const int nhi = engine_nhi(g);
+    if (nhi == 0) return FQ_ERR_INVALID;
+    const int n = kPhaseLo + nhi;
+    const int tok = prof_begin(ctx);
+    k_phase_table2<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ptab, (int)g.cmin, nhi,
+                                                              g.W_int, gamma, scale);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
+    ctx->launches++;
+    return FQ_OK;
 }
 
 static int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
@@ -481,13 +538,20 @@ int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph,
         double gx, f;
         gate_params(betas[p], gm, gx, f);
         const double scale = pow(f, N) * (p == 0 ? amp0 : 1.0);
-        if (g.integer) FQ_TRY(launch_table(ctx, g, gammas[p], scale));
+        const int nhi = g.integer ? engine_nhi(g) : 0;
+        if (g.integer) {
+            if (nhi > 0)
+                FQ_TRY(launch_table2(ctx, g, gammas[p], scale));
+            else
+                FQ_TRY(launch_table(ctx, g, gammas[p], scale));
+        }
         for (size_t i = 0; i < plan.size(); i++) {
             PassArgs A = base_args(ctx, sv, N, g);
             A.l = plan[i].l;
             A.a = plan[i].a;
             A.tmask = plan[i].tmask;
             A.gx = gx;
+            A.nhi = nhi;
             A.gamma = gammas[p];
             A.scale = g.integer ? 1.0 : scale;
             const int ph = i == 0 ? (p == 0 ? PH_INIT : PH_MUL) : PH_NONE;

@@ -69,13 +69,17 @@ enum { GM_NONE = 0, GM_TAN = 1, GM_COT = 2, GM_FULL = 3 };
 struct PassArgs {
     double2* sv;
     const void* w;        // N*N symmetric weights (int32 or float64), device
-    const double2* ptab;  // integer path: phase of cut value c at ptab[c - cmin]
+    // Integer path: the phase of cut value c.  nhi == 0: one table in global
+    // memory, ptab[c - cmin].  nhi > 0: two small tables copied to shared
+    // memory, ptab[0..32) = exp(i*gamma*j) and ptab[32 + h] = phase of
+    // cmin + 32h, so phase(c) = hi[(c - cmin) >> 5] * lo[(c - cmin) & 31].
+    const double2* ptab;
     double* partial;      // <C> partial sums, one per CTA
     double* diag;         // cut-value output (EX_DIAG)
     i64 ntiles;
     int N, l, a;
     unsigned tmask;  // RX targets among the 12 tile bits
-    int cmin, ntab;
+    int cmin, ntab, nhi;
     double gx;       // t or u of the reduced gate
     double c, s;     // cos, sin of angle/2 for GM_FULL
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
@@ -86,6 +90,31 @@ struct PassArgs {
 };
 
 __device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j : a + j - l; }
+
+constexpr int kPhaseLo = 32;     // low-part entries of the two-level phase table
+constexpr int kPhaseHiMax = 512; // high-part entries kept in shared memory at most
+
+// Shared-memory bytes reserved for the two-level phase table.
+__host__ __device__ inline size_t phase_smem_bytes() {
+    return sizeof(double2) * (kPhaseLo + kPhaseHiMax);
+}
+
+// Copy the two-level phase table into shared memory (all threads).
+__device__ __forceinline__ void load_phase_tables(const PassArgs& A, double2* smtab, int tid,
+                                                  int nthreads) {
+    if (A.nhi > 0)
+        for (int i = tid; i < kPhaseLo + A.nhi; i += nthreads) smtab[i] = A.ptab[i];
+}
+
+// Phase (times the layer's scale) of a cut value on the integer path.
+__device__ __forceinline__ double2 int_phase(const PassArgs& A, const double2* smtab, int cr) {
+    const int ti = min(max(cr - A.cmin, 0), A.ntab - 1);  // guards the table read only
+    if (A.nhi > 0) {
+        const double2 h = smtab[kPhaseLo + (ti >> 5)], lo = smtab[ti & 31];
+        return make_double2(h.x * lo.x - h.y * lo.y, h.x * lo.y + h.y * lo.x);
+    }
+    return __ldg(A.ptab + ti);
+}
 
 // Swizzled slot of tile index t in the exchange buffer.
 __device__ __forceinline__ int xslot(int t) { return t ^ ((t >> 4) & 7); }
@@ -159,6 +188,22 @@ __device__ __forceinline__ int lay_index(int tid, int r) {
     return (lane << 4) | (warp << 9) | r;
 }
 
+// Barrier of one 256-thread group (named barrier 1 + g; 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kPassThreads) : "memory");
+}
+
+// exchange() for one of several 256-thread groups of a CTA.
+template <int LF, int LT>
+__device__ __forceinline__ void exchange_g(double2 (&v)[kRegs], double2* buf, int gtid, int g) {
+    group_sync(g);
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(gtid, r))] = v[r];
+    group_sync(g);
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(gtid, r))];
+}
+
 template <int LF, int LT>
 __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid) {
     __syncthreads();  // previous readers of buf are done
@@ -173,7 +218,7 @@ __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int 
 template <typename WT>
 __host__ __device__ inline size_t pass_smem_bytes(int N) {
     return sizeof(double2) * kTile + sizeof(double) * 8 + sizeof(i64) * 32 + sizeof(int) * 24 +
-           sizeof(WT) * (N * N + 32 + 16 + 24 + 16);
+           sizeof(WT) * (N * N + 32 + 16 + 24 + 16) + 16 + phase_smem_bytes();
 }
 
 template <typename WT, int PH, int GM, int EX, bool ST, int SC>
@@ -190,6 +235,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     WT* creg = ke + 32;                                    // 16: cut among register bits
     WT* Dm = creg + 16;                                    // nF
     WT* Ru = Dm + 24;                                      // 12
+    double2* smtab = reinterpret_cast<double2*>(
+        (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);  // phase tables
     constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
     constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -208,6 +255,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
         if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
     }
+    if (PH != PH_NONE && sizeof(WT) == sizeof(int)) load_phase_tables(A, smtab, tid, kPassThreads);
     __syncthreads();
     if (CUT) {
         if (tid < nF) {
@@ -344,10 +392,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 double2 ph;
                 if (sizeof(WT) == sizeof(int)) {
-                    // The cut value lies in [cmin, cmin + ntab); the clamp only
-                    // guards the table read.
-                    const int ti = min(max((int)cr - A.cmin, 0), A.ntab - 1);
-                    ph = __ldg(A.ptab + ti);
+                    ph = int_phase(A, smtab, (int)cr);
                 } else {
                     const double S = 2.0 * (double)cr - A.W;
                     double sn, cs;
