@@ -62,6 +62,7 @@ SIGNATURES = {
     "fq_cut_diagonal": (_i, [_vp, _vp, _i, _dp]),
     "fq_permute_qubits": (_i, [_vp, _vp, _vp, _i, _ip]),
     "fq_reference_label_map": (_i, [_i, _i, _i, _ip]),
+    "fq_expectation_noalloc": (_i, [_vp, _i, _dp, _dp, _vp]),
 }
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(_lib, _name)

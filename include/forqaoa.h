@@ -133,6 +133,20 @@ int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph_upper
 int fq_cut_diagonal(fq_ctx* ctx, void* out, int N, const double* graph_upper);
 /* dst[y] = src[x], y having bit perm[b] equal to bit b of x (out of place). */
 int fq_permute_qubits(fq_ctx* ctx, const void* src, void* dst, int N, const int* perm);
+/* <C> of a device state without allocating any device memory, for callers
+ * that cannot call cudaMalloc (their device memory belongs to another
+ * allocator, or they cannot afford cudaMalloc's implicit synchronisation).
+ * No counterpart in the reference.  Needs no fq_ctx: sv is the caller's
+ * state, graph_upper the host graph, stream the caller's stream (NULL = the
+ * legacy default stream); writes *energy (host) and synchronises the stream.
+ * All scratch (weights, partial sums, result) lives in one fixed 32 KiB
+ * device array that every GPU loading the library keeps until exit; N must
+ * be in [2, 33].  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int fq_expectation_noalloc(const void* sv, int N, const double* graph_upper, double* energy,
+                           void* stream);
 /* Physical -> logical qubit map the reference schedule leaves after P layers
  * with chunk size C (src/Weighted.cpp:97-138): label_map[b] = logical qubit
  * at physical position b.  Host only. */
