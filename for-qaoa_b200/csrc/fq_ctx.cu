@@ -195,15 +195,16 @@ int fq_ctx_create(int device, void* stream, fq_ctx** out) {
         if (cudaMalloc(&c->d_w, wbytes) != cudaSuccess ||
             cudaMalloc(&c->d_ptab, sizeof(double2) * kMaxPhaseTable) != cudaSuccess ||
             cudaMalloc(&c->d_partial, sizeof(double) * c->partial_cap) != cudaSuccess ||
-            cudaMalloc(&c->d_result, sizeof(double) * 64) != cudaSuccess ||
+            cudaMalloc(&c->d_result, sizeof(double) * kResultWords) != cudaSuccess ||
+            cudaMalloc(&c->d_scratch, kScratchBytes) != cudaSuccess ||
             cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
             cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
             st = FQ_ERR_OOM;
             break;
         }
-        c->h_stage_bytes = std::max(wbytes, (size_t)64 * 1024);
+        c->h_stage_bytes = std::max(wbytes, (size_t)256 * 1024);
         if (cudaMallocHost(&c->h_stage, c->h_stage_bytes) != cudaSuccess ||
-            cudaMallocHost(&c->h_result, sizeof(double) * 64) != cudaSuccess) {
+            cudaMallocHost(&c->h_result, sizeof(double) * kResultWords) != cudaSuccess) {
             st = FQ_ERR_OOM;
             break;
         }
@@ -231,6 +232,7 @@ int fq_ctx_destroy(fq_ctx* c) {
     cudaFree(c->d_partial);
     cudaFree(c->d_result);
     cudaFree(c->d_err);
+    cudaFree(c->d_scratch);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->stage_evt) cudaEventDestroy(c->stage_evt);

@@ -15,7 +15,8 @@ struct fq_ctx {
     void* d_w = nullptr;          // N*N weights (int32 or float64)
     double2* d_ptab = nullptr;    // integer phase table
     double* d_partial = nullptr;  // per-CTA reduction partials
-    double* d_result = nullptr;   // small device results
+    double* d_result = nullptr;   // small device results (kResultWords)
+    unsigned char* d_scratch = nullptr;  // small-instance job data (kScratchBytes)
     int* d_err = nullptr;         // kernels' error flag (nonzero: a bounded wait gave up)
     int partial_cap = 0;
     // Pinned host staging (uploads of weights and small tables).
@@ -43,6 +44,9 @@ struct fq_ctx {
 };
 
 namespace fq {
+
+constexpr int kResultWords = 4096;
+constexpr size_t kScratchBytes = 1 << 20;
 
 // Host view of a graph, prepared for the kernels.
 struct GraphPrep {

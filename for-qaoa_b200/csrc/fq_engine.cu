@@ -7,11 +7,9 @@
 #include <algorithm>
 #include <vector>
 
-#include <cudaTypedefs.h>
-
 #include "fq_ctx.h"
-#include "fq_pass.cuh"
-#include "fq_pass_tma.cuh"
+#include "fq_engine.h"
+#include "fq_launch.cuh"
 
 namespace fq {
 
@@ -146,207 +144,8 @@ __global__ void k_cut_small(const double2* sv, int N, const double* w, double* e
     }
 }
 
-// ------------------------------------------------------------ pass launch --
-
-// Kind of a pass for profiling, and the HBM bytes it must move.
-template <int PH, int GM, int EX, bool ST>
-static int pass_kind() {
-    if (EX == EX_ENERGY && !ST) return FQ_KIND_EXPECT;
-    if (EX == EX_DIAG) return FQ_KIND_EXPECT;
-    if (GM == GM_FULL) return FQ_KIND_RX;
-    if (GM == GM_NONE) return FQ_KIND_COST;
-    return PH != PH_NONE ? FQ_KIND_LAYER_PASS : FQ_KIND_STRIDED_PASS;
-}
-
-template <int PH, int EX, bool ST>
-static double pass_bytes(int N) {
-    const double n = (double)(1ull << N);
-    const bool load = (PH != PH_INIT) && (ST || EX == EX_ENERGY);
-    return n * ((load ? 16.0 : 0.0) + (ST ? 16.0 : 0.0) + (EX == EX_DIAG ? 8.0 : 0.0));
-}
-
-template <typename WT, int PH, int GM, int EX, bool ST, int SC>
-static int launch_pass(fq_ctx* ctx, const PassArgs& A) {
-    auto fn = k_pass<WT, PH, GM, EX, ST, SC>;
-    const size_t smem = pass_smem_bytes<WT>(A.N);
-    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)pass_smem_bytes<WT>(kMaxQubits)));
-    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
-    const int tok = prof_begin(ctx);
-    fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A);
-    FQ_CUDA(cudaGetLastError());
-    prof_end(ctx, tok, pass_kind<PH, GM, EX, ST>(), pass_bytes<PH, EX, ST>(A.N));
-    ctx->launches++;
-    return FQ_OK;
-}
-
-// ------------------------------------------------------------ TMA pass --
-
-static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-        else
-            cudaGetLastError();
-    }
-    return fn;
-}
-
-// Which passes run as TMA pipelines (FQ_TMA overrides; measured on B200 at
-// N=30, see the profiles):
-//   0  none (every pass uses per-thread loads, k_pass)
-//   1  passes without a cost phase use the one-group TMA pass (default:
-//      strided passes are fastest there, the phase pass with k_pass)
-//   2  every read-write pass uses the two-group TMA pass
-//   3  every read-write pass uses the one-group TMA pass
-static int tma_mode() {
-    static int m = -1;
-    if (m < 0) {
-        const char* e = getenv("FQ_TMA");
-        m = e ? std::max(0, std::min(3, atoi(e))) : 1;
-    }
-    return m;
-}
-static bool tma_for(int ph) {
-    const int m = tma_mode();
-    return m >= 2 || (m == 1 && ph == PH_NONE);
-}
-static int tma_groups() { return tma_mode() == 2 ? 2 : 1; }
-
-// The state as a tensor of float64 whose innermost dimension is one 128-byte
-// row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
-// Returns false for tiles with rows narrower than 8 amplitudes.
-static bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G) {
-    auto enc = tmap_encoder();
-    if (!enc || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
-    const int N = A.N, l = A.l, a = A.a, k = kTileBits - l;
-    cuuint64_t dims[5];
-    cuuint64_t strides[4];
-    cuuint32_t box[5];
-    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
-    int rank;
-    if (l == kTileBits) {
-        rank = 3;
-        G->kind = TG_CONTIG;
-        dims[0] = 16; dims[1] = 256; dims[2] = 1ull << (N - 11);
-        strides[0] = 128; strides[1] = 128ull * 256;
-        box[0] = 16; box[1] = 256; box[2] = 2;
-    } else if (l >= 4 && l <= 11) {
-        rank = 5;
-        G->kind = TG_ROWS;
-        dims[0] = 16; dims[1] = 1ull << (l - 3); dims[2] = 1ull << (a - l);
-        dims[3] = 1ull << k; dims[4] = 1ull << (N - a - k);
-        strides[0] = 128; strides[1] = 16ull << l; strides[2] = 16ull << a;
-        strides[3] = 16ull << (a + k);
-        box[0] = 16; box[1] = 1u << (l - 3); box[2] = 1; box[3] = 1u << k; box[4] = 1;
-    } else if (l == 3) {
-        rank = 5;
-        G->kind = TG_ROWS8;
-        dims[0] = 16; dims[1] = 1ull << (a - 3); dims[2] = 32; dims[3] = 16;
-        dims[4] = 1ull << (N - a - 9);
-        strides[0] = 128; strides[1] = 16ull << a; strides[2] = 16ull << (a + 5);
-        strides[3] = 16ull << (a + 9);
-        box[0] = 16; box[1] = 1; box[2] = 32; box[3] = 16; box[4] = 1;
-    } else {
-        return false;
-    }
-    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, (void*)A.sv, dims, strides,
-                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
-
-template <typename WT, int PH, int GM, int EX, int SC>
-static int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, TmaGeom G) {
-    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
-    const int tok = prof_begin(ctx);
-    if (tma_groups() == 2) {
-        auto fn = k_pass_tma2<WT, PH, GM, EX, SC>;
-        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tma2_pass_smem_bytes<WT>(kMaxQubits)));
-        fn<<<(unsigned)grid, 2 * kPassThreads, tma2_pass_smem_bytes<WT>(A.N), ctx->stream>>>(
-            A, map, G);
-    } else {
-        auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
-        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
-        fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map,
-                                                                                        G);
-    }
-    FQ_CUDA(cudaGetLastError());
-    prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
-    ctx->launches++;
-    return FQ_OK;
-}
-
-// Passes without RX (cost phase, <C>, cut diagonal) use the L0 schedule.
-// Passes that read and write the state run as TMA pipelines where the tile
-// geometry allows; write-only (layer-0) and read-only passes use k_pass.
-template <typename WT, int PH, int GM, int EX, bool ST>
-static int launch_pass(fq_ctx* ctx, const PassArgs& A) {
-    if (GM == GM_NONE && !(ST && PH == PH_MUL)) return launch_pass<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
-    const int sc = GM == GM_NONE ? SC_L0 : schedule_for(A.tmask);
-    if (ST && PH != PH_INIT && EX != EX_DIAG && tma_for(PH)) {
-        alignas(64) CUtensorMap map;
-        TmaGeom G;
-        if (make_pass_tmap(A, &map, &G)) {
-            constexpr int EXT = EX == EX_ENERGY ? EX_ENERGY : EX_NONE;
-            switch (sc) {
-                case SC_L021: return launch_tma<WT, PH, GM, EXT, SC_L021>(ctx, A, map, G);
-                case SC_L01: return launch_tma<WT, PH, GM, EXT, SC_L01>(ctx, A, map, G);
-                default: return launch_tma<WT, PH, GM, EXT, SC_L0>(ctx, A, map, G);
-            }
-        }
-    }
-    switch (sc) {
-        case SC_L021: return launch_pass<WT, PH, GM, EX, ST, SC_L021>(ctx, A);
-        case SC_L01: return launch_pass<WT, PH, GM, EX, ST, SC_L01>(ctx, A);
-        default: return launch_pass<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
-    }
-}
-
-static int pass_grid(fq_ctx* ctx, const PassArgs& A) {
-    return (int)std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
-}
-
-// Whether launch_pass will run A as a TMA pipeline (one CTA per SM).
-static bool runs_as_tma(const PassArgs& A, int ph) {
-    if (!tma_for(ph) || ph == PH_INIT) return false;
-    if (!tmap_encoder() || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
-    return A.l >= 3;
-}
-
-template <typename WT, int PH, int EX>
-static int launch_gm(fq_ctx* ctx, int gm, const PassArgs& A) {
-    if (gm == GM_TAN) return launch_pass<WT, PH, GM_TAN, EX, true>(ctx, A);
-    return launch_pass<WT, PH, GM_COT, EX, true>(ctx, A);
-}
-
-template <typename WT>
-static int launch_engine_pass(fq_ctx* ctx, int ph, int gm, int ex, const PassArgs& A) {
-    if (ph == PH_INIT)
-        return ex ? launch_gm<WT, PH_INIT, EX_ENERGY>(ctx, gm, A)
-                  : launch_gm<WT, PH_INIT, EX_NONE>(ctx, gm, A);
-    if (ph == PH_MUL)
-        return ex ? launch_gm<WT, PH_MUL, EX_ENERGY>(ctx, gm, A)
-                  : launch_gm<WT, PH_MUL, EX_NONE>(ctx, gm, A);
-    return ex ? launch_gm<WT, PH_NONE, EX_ENERGY>(ctx, gm, A)
-              : launch_gm<WT, PH_NONE, EX_NONE>(ctx, gm, A);
-}
-
 // ------------------------------------------------------------- planning --
 
-struct PassPlan {
-    int l, a;
-    unsigned tmask;
-};
 
 static int passes_for(int N, int lrows) {
     return 1 + (N - kTileBits + (kTileBits - lrows) - 1) / (kTileBits - lrows);
@@ -369,7 +168,7 @@ static int choose_lrows(int N) {
 // One layer's passes: the contiguous tile 0..11 (cost phase + 12 RX), then
 // strided tiles bringing the next 12 - lrows qubits on chip each.  The last
 // strided pass widens its rows when fewer qubits remain.
-static std::vector<PassPlan> plan_layer(int N) {
+std::vector<PassPlan> plan_layer(int N) {
     std::vector<PassPlan> v;
     v.push_back({kTileBits, kTileBits, (1u << kTileBits) - 1});
     const int lrows = choose_lrows(N);
@@ -385,7 +184,7 @@ static std::vector<PassPlan> plan_layer(int N) {
 // Reduced RX: RX(beta) = f * G with G = [[1,-it],[-it,1]] (t = s/c, f = c)
 // or [[u,-i],[-i,u]] (u = c/s, f = s), whichever keeps |t|,|u| <= 1.  The
 // factor f of every gate in a layer is folded into that layer's phase.
-static void gate_params(double beta, int& gm, double& g, double& f) {
+void gate_params(double beta, int& gm, double& g, double& f) {
     const double s = sin(beta / 2), c = cos(beta / 2);
     if (fabs(c) >= fabs(s)) {
         gm = GM_TAN;
@@ -408,7 +207,7 @@ static int prefetch_distance() {
     return d;
 }
 
-static PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
+PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     PassArgs A;
     memset(&A, 0, sizeof(A));
     A.sv = (double2*)sv;
@@ -433,13 +232,13 @@ static PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
 
 // High-part entries of the engine's two-level phase table (0: the range is
 // too wide for shared memory and the one-level global table is used).
-static int engine_nhi(const GraphPrep& g) {
+int engine_nhi(const GraphPrep& g) {
     const long long range = g.cmax - g.cmin + 1;
     const long long nhi = (range + kPhaseLo - 1) / kPhaseLo;
     return nhi <= kPhaseHiMax ? (int)nhi : 0;
 }
 
-static int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
+int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
     const int nhi = engine_nhi(g);
     if (nhi == 0) return FQ_ERR_INVALID;
     const int n = kPhaseLo + nhi;
@@ -452,7 +251,7 @@ static int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double s
     return FQ_OK;
 }
 
-static int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
+int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
     const int n = (int)(g.cmax - g.cmin + 1);
     k_phase_table<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ptab, (int)g.cmin, n, g.W_int,
                                                              gamma, scale);
@@ -461,7 +260,7 @@ static int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double sc
     return FQ_OK;
 }
 
-static int read_result(fq_ctx* ctx, double* host) {
+int read_result(fq_ctx* ctx, double* host) {
     FQ_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, sizeof(double), cudaMemcpyDeviceToHost,
                             ctx->stream));
     FQ_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -470,14 +269,23 @@ static int read_result(fq_ctx* ctx, double* host) {
     return FQ_OK;
 }
 
-static int reduce_to_result(fq_ctx* ctx, int n) {
+int reduce_partials(fq_ctx* ctx, const double* partial, int n, double* out_dev) {
+    const int tok = prof_begin(ctx);
+    k_reduce_partials<<<1, 256, 0, ctx->stream>>>(partial, n, out_dev);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
+    ctx->launches++;
+    return FQ_OK;
+}
+
+int reduce_to_result(fq_ctx* ctx, int n) {
     k_reduce_partials<<<1, 256, 0, ctx->stream>>>(ctx->d_partial, n, ctx->d_result);
     FQ_CUDA(cudaGetLastError());
     ctx->launches++;
     return FQ_OK;
 }
 
-static int check_state(void* sv, int N) {
+int check_state(void* sv, int N) {
     FQ_CHECK(sv != nullptr, FQ_ERR_INVALID, "null state pointer");
     FQ_CHECK(((uintptr_t)sv & 15) == 0, FQ_ERR_INVALID, "state pointer not 16-byte aligned");
     FQ_CHECK(N >= 1 && N <= kMaxQubits, FQ_ERR_INVALID, "N=%d out of range [1,%d]", N, kMaxQubits);
@@ -485,10 +293,59 @@ static int check_state(void* sv, int N) {
 }
 
 // Prepare the graph; small states always use the FP64 weights.
-static int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g) {
+int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g) {
     FQ_TRY(prep_graph(graph, N, g));
     if (N < kTileBits) g.integer = false;
     FQ_TRY(upload_graph(ctx, g, graph));
+    return FQ_OK;
+}
+
+// The fused forward circuit for N >= 12 (see fq_qaoa_forward); with energy
+// != NULL the last sweep also sums <C> and *energy receives it.
+int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, const double* gammas,
+                   const double* betas, double* energy) {
+    const double amp0 = fq_init_amp(N);
+    const std::vector<PassPlan> plan = plan_layer(N);
+    int last_grid = 0;
+    for (int p = 0; p < P; p++) {
+        int gm;
+        double gx, f;
+        gate_params(betas[p], gm, gx, f);
+        const double scale = pow(f, N) * (p == 0 ? amp0 : 1.0);
+        const int nhi = g.integer ? engine_nhi(g) : 0;
+        if (g.integer) {
+            if (nhi > 0)
+                FQ_TRY(launch_table2(ctx, g, gammas[p], scale));
+            else
+                FQ_TRY(launch_table(ctx, g, gammas[p], scale));
+        }
+        for (size_t i = 0; i < plan.size(); i++) {
+            PassArgs A = base_args(ctx, sv, N, g);
+            A.l = plan[i].l;
+            A.a = plan[i].a;
+            A.tmask = plan[i].tmask;
+            A.gx = gx;
+            A.nhi = nhi;
+            A.gamma = gammas[p];
+            A.scale = g.integer ? 1.0 : scale;
+            const int ph = i == 0 ? (p == 0 ? PH_INIT : PH_MUL) : PH_NONE;
+            const int ex = (energy && p == P - 1 && i + 1 == plan.size() && i > 0) ? 1 : 0;
+            if (ph != PH_NONE)
+                FQ_TRY(dispatch_phase_pass(ctx, g.integer, ph, gm, A));
+            else
+                FQ_TRY(dispatch_rx(ctx, g.integer, gm, ex != 0, A));
+            last_grid = pass_grid(ctx, A, ph, true);
+        }
+    }
+    if (energy) {
+        if (plan.size() == 1) {  // the only pass carries the phase: <C> in its own sweep
+            PassArgs A = base_args(ctx, sv, N, g);
+            FQ_TRY(dispatch_readonly(ctx, g.integer, false, A));
+            last_grid = pass_grid(ctx, A, PH_NONE, false);
+        }
+        FQ_TRY(reduce_to_result(ctx, last_grid));
+        FQ_TRY(read_result(ctx, energy));
+    }
     return FQ_OK;
 }
 
@@ -531,44 +388,7 @@ int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph,
         }
         return FQ_OK;
     }
-    const std::vector<PassPlan> plan = plan_layer(N);
-    int last_grid = 0;
-    for (int p = 0; p < P; p++) {
-        int gm;
-        double gx, f;
-        gate_params(betas[p], gm, gx, f);
-        const double scale = pow(f, N) * (p == 0 ? amp0 : 1.0);
-        const int nhi = g.integer ? engine_nhi(g) : 0;
-        if (g.integer) {
-            if (nhi > 0)
-                FQ_TRY(launch_table2(ctx, g, gammas[p], scale));
-            else
-                FQ_TRY(launch_table(ctx, g, gammas[p], scale));
-        }
-        for (size_t i = 0; i < plan.size(); i++) {
-            PassArgs A = base_args(ctx, sv, N, g);
-            A.l = plan[i].l;
-            A.a = plan[i].a;
-            A.tmask = plan[i].tmask;
-            A.gx = gx;
-            A.nhi = nhi;
-            A.gamma = gammas[p];
-            A.scale = g.integer ? 1.0 : scale;
-            const int ph = i == 0 ? (p == 0 ? PH_INIT : PH_MUL) : PH_NONE;
-            const int ex = (energy && p == P - 1 && i + 1 == plan.size()) ? 1 : 0;
-            if (g.integer)
-                FQ_TRY(launch_engine_pass<int>(ctx, ph, gm, ex, A));
-            else
-                FQ_TRY(launch_engine_pass<double>(ctx, ph, gm, ex, A));
-            last_grid = runs_as_tma(A, ph) ? (int)std::min<i64>(A.ntiles, ctx->num_sms)
-                                           : pass_grid(ctx, A);
-        }
-    }
-    if (energy) {
-        FQ_TRY(reduce_to_result(ctx, last_grid));
-        FQ_TRY(read_result(ctx, energy));
-    }
-    return FQ_OK;
+    return engine_forward(ctx, sv, N, P, g, gammas, betas, energy);
 }
 
 int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph, double* energy) {
@@ -585,11 +405,8 @@ int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph, doub
         return read_result(ctx, energy);
     }
     PassArgs A = base_args(ctx, (void*)sv, N, g);
-    if (g.integer)
-        FQ_TRY((launch_pass<int, PH_NONE, GM_NONE, EX_ENERGY, false>(ctx, A)));
-    else
-        FQ_TRY((launch_pass<double, PH_NONE, GM_NONE, EX_ENERGY, false>(ctx, A)));
-    FQ_TRY(reduce_to_result(ctx, pass_grid(ctx, A)));
+    FQ_TRY(dispatch_readonly(ctx, g.integer, false, A));
+    FQ_TRY(reduce_to_result(ctx, pass_grid(ctx, A, PH_NONE, false)));
     return read_result(ctx, energy);
 }
 
@@ -608,9 +425,7 @@ int fq_cut_diagonal(fq_ctx* ctx, void* out, int N, const double* graph) {
     }
     PassArgs A = base_args(ctx, nullptr, N, g);
     A.diag = (double*)out;
-    if (g.integer)
-        return launch_pass<int, PH_NONE, GM_NONE, EX_DIAG, false>(ctx, A);
-    return launch_pass<double, PH_NONE, GM_NONE, EX_DIAG, false>(ctx, A);
+    return dispatch_readonly(ctx, g.integer, true, A);
 }
 
 // src/rzz.cu:173-206.  Layer 0 writes phase * init_amp (launch control,
@@ -634,11 +449,8 @@ int fq_cost_phase(fq_ctx* ctx, void* sv, int N, double angle, const double* grap
     A.scale = is_first_layer ? init_amp : 1.0;
     if (g.integer) {
         FQ_TRY(launch_table(ctx, g, angle, 1.0));
-        if (is_first_layer) return launch_pass<int, PH_INIT, GM_NONE, EX_NONE, true>(ctx, A);
-        return launch_pass<int, PH_MUL, GM_NONE, EX_NONE, true>(ctx, A);
     }
-    if (is_first_layer) return launch_pass<double, PH_INIT, GM_NONE, EX_NONE, true>(ctx, A);
-    return launch_pass<double, PH_MUL, GM_NONE, EX_NONE, true>(ctx, A);
+    return dispatch_phase_pass(ctx, g.integer, is_first_layer ? PH_INIT : PH_MUL, GM_NONE, A);
 }
 
 }  // extern "C"
@@ -668,7 +480,7 @@ static int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double
         A.tmask = (unsigned)(mask & 0xFFFull);
         A.c = c;
         A.s = s;
-        FQ_TRY((launch_pass<int, PH_NONE, GM_FULL, EX_NONE, true>(ctx, A)));
+        FQ_TRY(dispatch_rx_full(ctx, A));
     }
     unsigned long long rest = mask & ~0xFFFull;
     const int k = std::min(kTileBits - 3, N - kTileBits);
@@ -686,7 +498,7 @@ static int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double
             }
         A.c = c;
         A.s = s;
-        FQ_TRY((launch_pass<int, PH_NONE, GM_FULL, EX_NONE, true>(ctx, A)));
+        FQ_TRY(dispatch_rx_full(ctx, A));
     }
     return FQ_OK;
 }

@@ -1,0 +1,39 @@
+// fq_engine.h -- host-side pieces of the fused engine shared by the forward
+// circuit (fq_engine.cu) and the gradient (fq_grad.cu).
+#pragma once
+
+#include <vector>
+
+#include "fq_ctx.h"
+#include "fq_pass.cuh"
+
+namespace fq {
+
+// One pass of a layer: tile bits 0..l-1 = physical 0..l-1, tile bits
+// l..11 = physical a..a+11-l, RX on the tile bits of tmask.
+struct PassPlan {
+    int l, a;
+    unsigned tmask;
+};
+
+// Passes of one layer for N >= 12: the contiguous tile (phase + qubits
+// 0..11) first, then strided tiles over the remaining qubits.
+std::vector<PassPlan> plan_layer(int N);
+// Reduced RX for angle beta: gate mode, t or u, and the factor f.
+void gate_params(double beta, int& gm, double& g, double& f);
+PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g);
+// High-part entries of the two-level phase table (0: use the global table).
+int engine_nhi(const GraphPrep& g);
+int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
+int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
+// Fixed-order sum of n partials into one device word.
+int reduce_partials(fq_ctx* ctx, const double* partial, int n, double* out_dev);
+int reduce_to_result(fq_ctx* ctx, int n);
+// Copies ctx->d_result[0] to *host (synchronises).
+int read_result(fq_ctx* ctx, double* host);
+int check_state(void* sv, int N);
+int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g);
+int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, const double* gammas,
+                   const double* betas, double* energy);
+
+}  // namespace fq

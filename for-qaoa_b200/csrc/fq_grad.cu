@@ -1,0 +1,218 @@
+// fq_grad.cu -- <C> and its adjoint gradient with respect to every gamma_k
+// and beta_k in one forward and one reverse sweep (fq_qaoa_energy_grad), and
+// batches of small instances in one launch (fq_small_batch).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fq_ctx.h"
+#include "fq_engine.h"
+#include "fq_launch.cuh"
+#include "fq_pass_dual.cuh"
+#include "fq_small.cuh"
+
+namespace fq {
+
+template <typename WT, bool PHI, int SC>
+static int launch_dual(fq_ctx* ctx, const PassArgs& A, double* gb, double* gg) {
+    auto fn = k_pass_dual<WT, PHI, SC, true>;
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dual_smem_bytes<WT>(kMaxQubits)));
+    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
+    const int tok = prof_begin(ctx);
+    fn<<<(unsigned)grid, kPassThreads, dual_smem_bytes<WT>(A.N), ctx->stream>>>(A, gb, gg);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, FQ_KIND_ADJOINT, 64.0 * (double)(1ull << A.N));
+    ctx->launches++;
+    return FQ_OK;
+}
+
+static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, const PassArgs& A, double* gb,
+                         double* gg) {
+    if (phi) {
+        FQ_CHECK(schedule_for(A.tmask) == SC_L021, FQ_ERR_INVALID, "adjoint phase pass mask");
+        return integer ? launch_dual<int, true, SC_L021>(ctx, A, gb, gg)
+                       : launch_dual<double, true, SC_L021>(ctx, A, gb, gg);
+    }
+    switch (schedule_for(A.tmask)) {
+        case SC_L021: return launch_dual<int, false, SC_L021>(ctx, A, gb, gg);
+        case SC_L01: return launch_dual<int, false, SC_L01>(ctx, A, gb, gg);
+        default: return launch_dual<int, false, SC_L0>(ctx, A, gb, gg);
+    }
+}
+
+// Upload a batch of small jobs (descriptors + their data) through the
+// pinned staging buffer into ctx->d_scratch and launch one CTA per job.
+// data: per job, N*N weights, P gammas, P betas (doubles, host); outputs go
+// to d_result starting at word out_base.
+struct SmallHostJob {
+    int N, P, flags;
+    const double* w;  // N*N symmetric (host)
+    const double* gammas;
+    const double* betas;
+    double2* state;   // device or null
+};
+
+static int run_small_jobs(fq_ctx* ctx, const SmallHostJob* jobs, int njobs, int out_base,
+                          std::vector<int>& out_off) {
+    size_t need = sizeof(SmallJob) * njobs;
+    int nmax = 1, outw = 0;
+    for (int i = 0; i < njobs; i++) {
+        need += sizeof(double) * (jobs[i].N * jobs[i].N + 2 * jobs[i].P);
+        nmax = std::max(nmax, jobs[i].N);
+        outw += 1 + 2 * jobs[i].P;
+    }
+    FQ_CHECK(need <= ctx->h_stage_bytes && need <= kScratchBytes, FQ_ERR_INVALID,
+             "small batch too large for the staging buffer (%zu bytes)", need);
+    FQ_CHECK(out_base + outw <= kResultWords, FQ_ERR_INVALID, "too many small-job outputs");
+    FQ_TRY(stage_acquire(ctx));
+    unsigned char* h = ctx->h_stage;
+    SmallJob* hj = reinterpret_cast<SmallJob*>(h);
+    double* hd = reinterpret_cast<double*>(h + sizeof(SmallJob) * njobs);
+    const double* dd = reinterpret_cast<const double*>(ctx->d_scratch + sizeof(SmallJob) * njobs);
+    size_t off = 0;
+    int o = out_base;
+    out_off.assign(njobs, 0);
+    for (int i = 0; i < njobs; i++) {
+        const SmallHostJob& J = jobs[i];
+        SmallJob d;
+        d.N = J.N;
+        d.P = J.P;
+        d.flags = J.flags;
+        d.pad = 0;
+        memcpy(hd + off, J.w, sizeof(double) * J.N * J.N);
+        d.w = dd + off;
+        off += J.N * J.N;
+        memcpy(hd + off, J.gammas, sizeof(double) * J.P);
+        d.gammas = dd + off;
+        off += J.P;
+        memcpy(hd + off, J.betas, sizeof(double) * J.P);
+        d.betas = dd + off;
+        off += J.P;
+        d.out = ctx->d_result + o;
+        out_off[i] = o;
+        o += 1 + 2 * J.P;
+        d.state = J.state;
+        hj[i] = d;
+    }
+    FQ_CUDA(cudaMemcpyAsync(ctx->d_scratch, h, need, cudaMemcpyHostToDevice, ctx->stream));
+    FQ_CUDA(cudaEventRecord(ctx->stage_evt, ctx->stream));
+    const size_t smem = small_smem_bytes(nmax);
+    FQ_CUDA(cudaFuncSetAttribute(k_small_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)small_smem_bytes(kSmallMaxQubits)));
+    const int tok = prof_begin(ctx);
+    k_small_jobs<<<njobs, kSmallThreads, smem, ctx->stream>>>(
+        reinterpret_cast<const SmallJob*>(ctx->d_scratch), njobs);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
+    ctx->launches++;
+    return FQ_OK;
+}
+
+static int read_results(fq_ctx* ctx, int words) {
+    FQ_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, sizeof(double) * words,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    return check_device_error(ctx);
+}
+
+static int check_angles(int P, const double* gammas, const double* betas) {
+    FQ_CHECK(P >= 1 && gammas && betas, FQ_ERR_INVALID, "need P >= 1 and angle arrays");
+    for (int p = 0; p < P; p++)
+        FQ_CHECK(isfinite(gammas[p]) && isfinite(betas[p]), FQ_ERR_INVALID,
+                 "non-finite angle at layer %d", p);
+    return FQ_OK;
+}
+
+}  // namespace fq
+
+using namespace fq;
+
+extern "C" {
+
+int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, const double* graph,
+                        const double* gammas, const double* betas, double* energy,
+                        double* grad_gamma, double* grad_beta) {
+    FQ_TRY(validate_ctx(ctx));
+    FQ_CHECK(N >= 2 && N <= kMaxQubits, FQ_ERR_INVALID, "N=%d out of range [2,%d]", N,
+             kMaxQubits);
+    FQ_TRY(check_angles(P, gammas, betas));
+    FQ_CHECK(energy && grad_gamma && grad_beta, FQ_ERR_INVALID, "null output");
+    if (N <= kSmallMaxQubits) {
+        FQ_CHECK(1 + 2 * P <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
+        GraphPrep g;
+        FQ_TRY(prep_graph(graph, N, g));
+        SmallHostJob J{N, P, SJ_ENERGY | SJ_GRAD, g.wd.data(), gammas, betas, nullptr};
+        std::vector<int> off;
+        FQ_TRY(run_small_jobs(ctx, &J, 1, 0, off));
+        FQ_TRY(read_results(ctx, 1 + 2 * P));
+        *energy = ctx->h_result[0];
+        for (int k = 0; k < P; k++) {
+            grad_gamma[k] = ctx->h_result[1 + k];
+            grad_beta[k] = ctx->h_result[1 + P + k];
+        }
+        return FQ_OK;
+    }
+    FQ_TRY(check_state(sv, N));
+    FQ_TRY(check_state(costate, N));
+    FQ_CHECK(sv != costate, FQ_ERR_INVALID, "state and costate must be different buffers");
+    GraphPrep g;
+    FQ_TRY(setup_graph(ctx, graph, N, g));
+    const std::vector<PassPlan> plan = plan_layer(N);
+    const int npass = (int)plan.size();
+    FQ_CHECK(1 + P + P * npass <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
+
+    // Forward circuit, then lambda = C psi with <C>.
+    FQ_TRY(engine_forward(ctx, sv, N, P, g, gammas, betas, nullptr));
+    {
+        PassArgs A = base_args(ctx, sv, N, g);
+        A.sv2 = (double2*)costate;
+        FQ_TRY(dispatch_costate(ctx, g.integer, A));
+        FQ_TRY(reduce_partials(ctx, ctx->d_partial, pass_grid(ctx, A, PH_NONE, false),
+                               ctx->d_result));
+    }
+    // Reverse sweep: per layer the strided passes, then the contiguous pass
+    // with dE/dgamma and the inverse phase.
+    double* gb = ctx->d_partial;
+    for (int k = P - 1; k >= 0; k--) {
+        const int nhi = g.integer ? engine_nhi(g) : 0;
+        if (g.integer) {
+            if (nhi > 0)
+                FQ_TRY(launch_table2(ctx, g, gammas[k], 1.0));
+            else
+                FQ_TRY(launch_table(ctx, g, gammas[k], 1.0));
+        }
+        for (int o = 1; o <= npass; o++) {
+            const int i = o % npass;  // 1, 2, ..., npass-1, then 0
+            PassArgs A = base_args(ctx, sv, N, g);
+            A.sv2 = (double2*)costate;
+            A.l = plan[i].l;
+            A.a = plan[i].a;
+            A.tmask = plan[i].tmask;
+            A.c = cos(betas[k] / 2);
+            A.s = -sin(betas[k] / 2);  // RX(-beta)
+            A.gamma = gammas[k];
+            A.nhi = nhi;
+            A.scale = k > 0 ? 1.0 : 0.0;  // inverse phase only where layers remain
+            const int grid = (int)std::min<i64>(A.ntiles, ctx->num_sms);
+            double* gg = gb + grid;
+            FQ_TRY(dispatch_dual(ctx, g.integer, i == 0, A, gb, gg));
+            FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + 1 + P + k * npass + i));
+            if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
+        }
+    }
+    FQ_TRY(read_results(ctx, 1 + P + P * npass));
+    const double* r = ctx->h_result;
+    *energy = r[0];
+    for (int k = 0; k < P; k++) {
+        grad_gamma[k] = -r[1 + k];
+        double s = 0;
+        for (int i = 0; i < npass; i++) s += r[1 + P + k * npass + i];
+        grad_beta[k] = s;
+    }
+    return FQ_OK;
+}
+
+}  // extern "C"

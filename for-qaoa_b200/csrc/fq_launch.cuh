@@ -1,0 +1,225 @@
+// fq_launch.cuh -- host-side launch of the tile passes (k_pass, k_pass_tma,
+// k_pass_tma2): schedule selection, TMA tensor maps, profiling brackets.
+// The kernel variants are instantiated in a few translation units
+// (fq_disp_*.cu) so they compile in parallel; fq_engine.cu calls the
+// dispatch_* entry points declared at the end.
+#pragma once
+
+#include <cudaTypedefs.h>
+#include <stdlib.h>
+
+#include <algorithm>
+
+#include "fq_ctx.h"
+#include "fq_pass.cuh"
+#include "fq_pass_tma.cuh"
+
+namespace fq {
+
+// Kind of a pass for profiling, and the HBM bytes it must move.
+template <int PH, int GM, int EX, bool ST>
+inline int pass_kind() {
+    if ((EX == EX_ENERGY || EX == EX_COSTATE) && !ST) return FQ_KIND_EXPECT;
+    if (EX == EX_DIAG) return FQ_KIND_EXPECT;
+    if (GM == GM_FULL) return FQ_KIND_RX;
+    if (GM == GM_NONE) return FQ_KIND_COST;
+    return PH != PH_NONE ? FQ_KIND_LAYER_PASS : FQ_KIND_STRIDED_PASS;
+}
+
+template <int PH, int EX, bool ST>
+inline double pass_bytes(int N) {
+    const double n = (double)(1ull << N);
+    const bool load = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
+    return n * ((load ? 16.0 : 0.0) + (ST ? 16.0 : 0.0) + (EX == EX_DIAG ? 8.0 : 0.0) +
+                (EX == EX_COSTATE ? 16.0 : 0.0));
+}
+
+template <typename WT, int PH, int GM, int EX, bool ST, int SC>
+inline int launch_ldg(fq_ctx* ctx, const PassArgs& A) {
+    auto fn = k_pass<WT, PH, GM, EX, ST, SC>;
+    const size_t smem = pass_smem_bytes<WT>(A.N);
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pass_smem_bytes<WT>(kMaxQubits)));
+    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
+    const int tok = prof_begin(ctx);
+    fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, pass_kind<PH, GM, EX, ST>(), pass_bytes<PH, EX, ST>(A.N));
+    ctx->launches++;
+    return FQ_OK;
+}
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Which passes run as TMA pipelines (FQ_TMA overrides; measured on B200 at
+// N=30, see the profiles):
+//   0  none (every pass uses per-thread loads, k_pass)
+//   1  passes without a cost phase use the one-group TMA pass (default:
+//      strided passes are fastest there, the phase pass with k_pass)
+//   2  every read-write pass uses the two-group TMA pass (<C> passes the
+//      one-group one)
+//   3  every read-write pass uses the one-group TMA pass
+inline int tma_mode() {
+    static int m = -1;
+    if (m < 0) {
+        const char* e = getenv("FQ_TMA");
+        m = e ? std::max(0, std::min(3, atoi(e))) : 1;
+    }
+    return m;
+}
+inline bool tma_for(int ph) {
+    const int m = tma_mode();
+    return m >= 2 || (m == 1 && ph == PH_NONE);
+}
+
+// The state as a tensor of float64 whose innermost dimension is one 128-byte
+// row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
+// Returns false for tiles with rows narrower than 8 amplitudes.
+inline bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G) {
+    auto enc = tmap_encoder();
+    if (!enc || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
+    const int N = A.N, l = A.l, a = A.a, k = kTileBits - l;
+    cuuint64_t dims[5];
+    cuuint64_t strides[4];
+    cuuint32_t box[5];
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    int rank;
+    if (l == kTileBits) {
+        rank = 3;
+        G->kind = TG_CONTIG;
+        dims[0] = 16; dims[1] = 256; dims[2] = 1ull << (N - 11);
+        strides[0] = 128; strides[1] = 128ull * 256;
+        box[0] = 16; box[1] = 256; box[2] = 2;
+    } else if (l >= 4 && l <= 11) {
+        rank = 5;
+        G->kind = TG_ROWS;
+        dims[0] = 16; dims[1] = 1ull << (l - 3); dims[2] = 1ull << (a - l);
+        dims[3] = 1ull << k; dims[4] = 1ull << (N - a - k);
+        strides[0] = 128; strides[1] = 16ull << l; strides[2] = 16ull << a;
+        strides[3] = 16ull << (a + k);
+        box[0] = 16; box[1] = 1u << (l - 3); box[2] = 1; box[3] = 1u << k; box[4] = 1;
+    } else if (l == 3) {
+        rank = 5;
+        G->kind = TG_ROWS8;
+        dims[0] = 16; dims[1] = 1ull << (a - 3); dims[2] = 32; dims[3] = 16;
+        dims[4] = 1ull << (N - a - 9);
+        strides[0] = 128; strides[1] = 16ull << a; strides[2] = 16ull << (a + 5);
+        strides[3] = 16ull << (a + 9);
+        box[0] = 16; box[1] = 1; box[2] = 32; box[3] = 16; box[4] = 1;
+    } else {
+        return false;
+    }
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, (void*)A.sv, dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <typename WT, int PH, int GM, int EX, int SC>
+inline int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, TmaGeom G) {
+    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
+    const int tok = prof_begin(ctx);
+    bool launched = false;
+    if constexpr (EX == EX_NONE) {
+        if (tma_mode() == 2) {
+            auto fn = k_pass_tma2<WT, PH, GM, EX, SC>;
+            FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)tma2_pass_smem_bytes<WT>(kMaxQubits)));
+            fn<<<(unsigned)grid, 2 * kPassThreads, tma2_pass_smem_bytes<WT>(A.N),
+                 ctx->stream>>>(A, map, G);
+            launched = true;
+        }
+    }
+    if (!launched) {
+        auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
+        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
+        fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map,
+                                                                                        G);
+    }
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
+    ctx->launches++;
+    return FQ_OK;
+}
+
+// Launch one pass with the round schedule its target mask needs.  Passes
+// without RX (cost phase, <C>, cut diagonal) use the L0 schedule.  Passes
+// that read and write the state run as TMA pipelines where tma_for() and
+// the tile geometry allow; write-only (layer-0) and read-only passes use
+// k_pass.
+template <typename WT, int PH, int GM, int EX, bool ST>
+inline int launch_pass(fq_ctx* ctx, const PassArgs& A) {
+    if constexpr (ST && PH != PH_INIT && EX != EX_DIAG && EX != EX_COSTATE) {
+        if (tma_for(PH)) {
+            alignas(64) CUtensorMap map;
+            TmaGeom G;
+            if (make_pass_tmap(A, &map, &G)) {
+                if constexpr (GM == GM_NONE) {
+                    return launch_tma<WT, PH, GM, EX, SC_L0>(ctx, A, map, G);
+                } else {
+                    switch (schedule_for(A.tmask)) {
+                        case SC_L021: return launch_tma<WT, PH, GM, EX, SC_L021>(ctx, A, map, G);
+                        case SC_L01: return launch_tma<WT, PH, GM, EX, SC_L01>(ctx, A, map, G);
+                        default: return launch_tma<WT, PH, GM, EX, SC_L0>(ctx, A, map, G);
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (GM == GM_NONE) {
+        return launch_ldg<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
+    } else {
+        switch (schedule_for(A.tmask)) {
+            case SC_L021: return launch_ldg<WT, PH, GM, EX, ST, SC_L021>(ctx, A);
+            case SC_L01: return launch_ldg<WT, PH, GM, EX, ST, SC_L01>(ctx, A);
+            default: return launch_ldg<WT, PH, GM, EX, ST, SC_L0>(ctx, A);
+        }
+    }
+}
+
+// Grid (and <C> partial count) of a pass launched by launch_pass.
+inline int pass_grid(fq_ctx* ctx, const PassArgs& A, int ph, bool st) {
+    const bool tma = st && ph != PH_INIT && tma_for(ph) && tmap_encoder() && A.sv &&
+                     ((uintptr_t)A.sv & 127) == 0 && A.l >= 3;
+    const i64 per = tma ? 1 : ctx->ctas_per_sm;
+    return (int)std::min<i64>(A.ntiles, per * ctx->num_sms);
+}
+
+// ---- dispatch entry points (one translation unit each) -------------------
+
+// Layer pass with a cost phase (ph = PH_INIT or PH_MUL) and RX on A.tmask
+// (gm = GM_TAN or GM_COT), or the cost phase alone (gm = GM_NONE).
+int dispatch_phase_pass(fq_ctx* ctx, bool integer, int ph, int gm, const PassArgs& A);
+// RX on A.tmask without a phase (reduced gates), optionally with <C>.
+int dispatch_rx_tan(fq_ctx* ctx, bool integer, bool energy, const PassArgs& A);
+int dispatch_rx_cot(fq_ctx* ctx, bool integer, bool energy, const PassArgs& A);
+// RX with the full formula of src/rx.cu:47-50 (reference-path kernels).
+int dispatch_rx_full(fq_ctx* ctx, const PassArgs& A);
+// Read-only sweeps: <C> partials or the cut diagonal (diag != 0).
+int dispatch_readonly(fq_ctx* ctx, bool integer, bool diag, const PassArgs& A);
+// <C> partials and the costate A.sv2 = C * A.sv.
+int dispatch_costate(fq_ctx* ctx, bool integer, const PassArgs& A);
+
+inline int dispatch_rx(fq_ctx* ctx, bool integer, int gm, bool energy, const PassArgs& A) {
+    if (gm == GM_TAN) return dispatch_rx_tan(ctx, integer, energy, A);
+    if (gm == GM_COT) return dispatch_rx_cot(ctx, integer, energy, A);
+    return dispatch_rx_full(ctx, A);
+}
+
+}  // namespace fq

@@ -51,7 +51,8 @@ constexpr int kMaxFixed = kMaxQubits - kTileBits;  // 21
 // Phase modes
 enum { PH_NONE = 0, PH_MUL = 1, PH_INIT = 2 };
 // Extra outputs: none, <C> partial sums, cut value of every amplitude
-enum { EX_NONE = 0, EX_ENERGY = 1, EX_DIAG = 2 };
+enum { EX_NONE = 0, EX_ENERGY = 1, EX_DIAG = 2, EX_COSTATE = 3 };
+// EX_COSTATE: <C> partial sums and the costate lambda = C psi written to sv2.
 // Round schedules: L0 only; L0 -> L1; L0 -> L2 -> L1 (see header comment).
 enum { SC_L0 = 0, SC_L01 = 1, SC_L021 = 2 };
 
@@ -68,6 +69,7 @@ enum { GM_NONE = 0, GM_TAN = 1, GM_COT = 2, GM_FULL = 3 };
 
 struct PassArgs {
     double2* sv;
+    double2* sv2;         // second vector: costate output (EX_COSTATE)
     const void* w;        // N*N symmetric weights (int32 or float64), device
     // Integer path: the phase of cut value c.  nhi == 0: one table in global
     // memory, ptab[c - cmin].  nhi > 0: two small tables copied to shared
@@ -238,7 +240,8 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     double2* smtab = reinterpret_cast<double2*>(
         (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);  // phase tables
     constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
-    constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY);
+    constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
+    constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
 
@@ -440,13 +443,17 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 __stcs(A.diag + base + thr_off + offtab[r], (double)cr);
             }
         }
-        if (EX == EX_ENERGY) {
+        if (ACC) {
             double ts = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
+                if (EX == EX_COSTATE) {
+                    const double c = (double)cr;
+                    __stcs(A.sv2 + base + thr_off + offtab[r], make_double2(c * v[r].x, c * v[r].y));
+                }
             }
             const double y = ts - comp;
             const double t2 = acc + y;
@@ -464,7 +471,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             }
         }
     }
-    if (EX == EX_ENERGY) {
+    if (ACC) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         __syncthreads();

@@ -19,7 +19,7 @@ OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BUSY = ran
 
 # Kernel kinds of fq_ctx_profile (include/forqaoa.h)
 KINDS = {"layer_pass": 0, "strided_pass": 1, "cost": 2, "rx": 3, "swap": 4, "expect": 5,
-         "other": 6}
+         "other": 6, "adjoint": 7}
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("libforqaoa.so not built: run `make -C for-qaoa_b200` "
@@ -59,6 +59,7 @@ SIGNATURES = {
     "fq_relabel_graph": (_i, [_dp, _i, _i, _i, _i]),
     "fq_qaoa_forward": (_i, [_vp, _vp, _i, _i, _dp, _dp, _dp, _dp]),
     "fq_expectation": (_i, [_vp, _vp, _i, _dp, _dp]),
+    "fq_qaoa_energy_grad": (_i, [_vp, _vp, _vp, _i, _i, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fq_cut_diagonal": (_i, [_vp, _vp, _i, _dp]),
     "fq_permute_qubits": (_i, [_vp, _vp, _vp, _i, _ip]),
     "fq_reference_label_map": (_i, [_i, _i, _i, _ip]),
@@ -246,6 +247,32 @@ class Context:
                                     _dptr(be), _dptr(e) if energy else None),
                "fq_qaoa_forward")
         return float(e[0]) if energy else None
+
+    def energy_grad(self, n, graph, gammas, betas, sv=None, costate=None):
+        """(<C>, dE/dgamma[P], dE/dbeta[P]) by the adjoint method.  sv and
+        costate are DeviceState workspaces of n qubits (allocated here when
+        omitted and n > 12)."""
+        g = _f64(graph)
+        ga, be = _f64(gammas), _f64(betas)
+        P = len(ga)
+        e, gg, gb = np.zeros(1), np.zeros(P), np.zeros(P)
+        own = []
+        if n > 12:
+            if sv is None:
+                sv = DeviceState(self, n)
+                own.append(sv)
+            if costate is None:
+                costate = DeviceState(self, n)
+                own.append(costate)
+        try:
+            _check(_lib.fq_qaoa_energy_grad(self.handle, sv.ptr if sv else None,
+                                            costate.ptr if costate else None, n, P, _dptr(g),
+                                            _dptr(ga), _dptr(be), _dptr(e), _dptr(gg),
+                                            _dptr(gb)), "fq_qaoa_energy_grad")
+        finally:
+            for s in own:
+                s.free()
+        return float(e[0]), gg, gb
 
     def expectation(self, st, graph):
         g = _f64(graph)

@@ -72,7 +72,8 @@ int fq_ctx_device_info(fq_ctx* ctx, int* num_sms, int* ctas_per_sm);
 #define FQ_KIND_RX 3            /* fq_rx_chunk / fq_rx_targets */
 #define FQ_KIND_SWAP 4          /* fq_swap_blocks */
 #define FQ_KIND_EXPECT 5        /* <C> / cut diagonal sweeps */
-#define FQ_KIND_OTHER 6         /* tables, reductions, permutations */
+#define FQ_KIND_OTHER 6         /* tables, reductions, permutations, small instances */
+#define FQ_KIND_ADJOINT 7       /* reverse-sweep passes over state and costate */
 #define FQ_KIND_COUNT 8
 int fq_ctx_set_profiling(fq_ctx* ctx, int enable);
 int fq_ctx_profile(fq_ctx* ctx, int kind, double* total_ms, long long* launches,
@@ -126,6 +127,18 @@ int fq_relabel_graph(double* graph_upper, int N, int swap_out, int swap_in,
  * synchronises the stream. */
 int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph_upper,
                     const double* gammas, const double* betas, double* energy);
+/* <C> and its gradient with respect to every gamma_k and beta_k of the
+ * P-layer circuit from |+>^N, by adjoint differentiation: one forward sweep,
+ * lambda = C psi, and one reverse sweep that moves psi and lambda back
+ * through the exact inverse of each layer (no stored intermediate states):
+ *   dE/dbeta_k = Im <lambda|sum_q X_q|psi>,  dE/dgamma_k = -Im <lambda|S|psi>.
+ * sv and costate are device workspaces of 2^N amplitudes each (contents
+ * unspecified on return; unused, may be NULL, for N <= 12, where the whole
+ * instance runs in one CTA's shared memory).  Writes *energy, grad_gamma[P],
+ * grad_beta[P] (host) and synchronises. */
+int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P,
+                        const double* graph_upper, const double* gammas, const double* betas,
+                        double* energy, double* grad_gamma, double* grad_beta);
 /* <C> of a state (read-only sweep).  Writes *energy (host); synchronises. */
 int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph_upper,
                    double* energy);

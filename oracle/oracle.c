@@ -191,18 +191,35 @@ void orc_weighted_run(int N, int C, int P, const double* graph_upper,
     free(lab);
 }
 
+/* The circuit in logical order.  S(z) is the pair-order sum of
+ * rzz.cu:131-143, computed once (it does not change between layers without
+ * relabelling); each layer then applies rzz.cu:146-154 and the mixer. */
 void orc_qaoa_logical(int N, int P, const double* graph_upper, const double* gammas,
                       const double* betas, double* sv) {
-    double* g1d = (double*)malloc(sizeof(double) * (N * (N - 1) / 2 + 1));
+    const i64 n = 1ll << N;
+    double* S = (double*)malloc(sizeof(double) * n);
     int targets[64];
     for (int q = 0; q < N; q++) targets[q] = q;
-    orc_upper_tri_to_1d(N, graph_upper, g1d);
+    orc_cost_diag_S(N, graph_upper, S);
     const double init_amp = orc_init_amp(N);
     for (int p = 0; p < P; p++) {
-        orc_cost_phase(sv, N, gammas[p], g1d, p == 0, init_amp);
+        const double angle = gammas[p];
+#pragma omp parallel for schedule(static)
+        for (i64 b = 0; b < n; b++) {
+            double s, c;
+            sincos(S[b] * angle / 2, &s, &c);
+            if (p == 0) {
+                sv[2 * b] = c * init_amp;
+                sv[2 * b + 1] = s * init_amp;
+            } else {
+                double re = sv[2 * b], im = sv[2 * b + 1];
+                sv[2 * b] = re * c - im * s;
+                sv[2 * b + 1] = re * s + im * c;
+            }
+        }
         orc_multi_rotate_x(sv, N, targets, N, betas[p]);
     }
-    free(g1d);
+    free(S);
 }
 
 void orc_cost_diag_S(int N, const double* graph_upper, double* S) {
