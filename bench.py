@@ -67,6 +67,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ref-schedule", action="store_true")
     ap.add_argument("--cpu-slice-bits", type=int, default=24)
+    ap.add_argument("--serve-requests", type=int, default=1000,
+                    help="requests of the served-stream leg (0: skip it)")
+    ap.add_argument("--serve-lanes", type=int, default=4)
     return ap.parse_args(argv)
 
 
@@ -379,6 +382,9 @@ def run_ours(args):
     if not args.no_ref_schedule:
         line["reference_schedule"] = reference_schedule_leg(ctx, args, graphs[0], gammas, betas,
                                                             peak)
+    # ---- served energy+gradient stream vs sequential plain calls (one GPU)
+    if args.serve_requests > 0 and d.world == 1:
+        line["serving"] = serving_leg(args)
     # ---- CPU baseline (rank 0, one GPU only)
     if not args.no_cpu and d.world == 1 and d.rank == 0:
         line["cpu_baseline"] = cpu_baseline_obj(args, graphs[0], gammas[0], betas[0])
@@ -386,6 +392,25 @@ def run_ours(args):
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.close()
+
+
+def serving_leg(args):
+    """A scaled sample of the served stream (sessions of 20 energy+gradient
+    steps, N ~ U{10..28}, p ~ U{1..8}, G(N,0.5) integer weights, Poisson
+    session arrivals, 150 GB budget): evals/s and p50/p99 latency through the
+    server, against the same evaluations as sequential plain calls."""
+    import forqaoa
+    import serve_stream as ss
+    sessions, steps = ss.make_stream(args.serve_requests, seed=5)
+    ss.run_served(forqaoa, sessions[:2], 1, lanes=args.serve_lanes)  # warm-up
+    served, wall, stats = ss.run_served(forqaoa, sessions, steps, lanes=args.serve_lanes)
+    seq, wall_q = ss.run_sequential(forqaoa, sessions, steps)
+    out = ss.summarize(served, wall, seq, wall_q, stats)
+    out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [10, 28], "p": [1, 8],
+                     "graph": "G(N,0.5), integer weights 1..10", "seed": 5,
+                     "arrivals": "Poisson, mean gap 1 ms", "lanes": args.serve_lanes,
+                     "budget_gb": 150, "sample_of": "10,000-request stream"}
+    return out
 
 
 def reference_schedule_leg(ctx, args, graph, gammas, betas, peak, steps=2):

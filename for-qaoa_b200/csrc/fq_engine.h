@@ -6,6 +6,7 @@
 
 #include "fq_ctx.h"
 #include "fq_pass.cuh"
+#include "fq_small.h"
 
 namespace fq {
 
@@ -35,5 +36,17 @@ int check_state(void* sv, int N);
 int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g);
 int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, const double* gammas,
                    const double* betas, double* energy);
+
+// The N >= 13 gradient split for asynchronous use: grad_enqueue puts every
+// kernel and the final device-to-host copy of the results on ctx's stream;
+// once the stream has passed that point, grad_collect assembles them.
+int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const double* graph,
+                 const double* gammas, const double* betas);
+int grad_collect(fq_ctx* ctx, int N, int P, double* energy, double* grad_gamma,
+                 double* grad_beta);
+
+// One CTA per job of k_small_jobs (fq_small.cuh); nmax = largest N.
+
+int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream);
 
 }  // namespace fq

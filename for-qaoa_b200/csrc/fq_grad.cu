@@ -43,6 +43,14 @@ static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, const PassArgs& A,
     }
 }
 
+int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream) {
+    FQ_CUDA(cudaFuncSetAttribute(k_small_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)small_smem_bytes(kSmallMaxQubits)));
+    k_small_jobs<<<njobs, kSmallThreads, small_smem_bytes(nmax), stream>>>(jobs, njobs);
+    FQ_CUDA(cudaGetLastError());
+    return FQ_OK;
+}
+
 // Upload a batch of small jobs (descriptors + their data) through the
 // pinned staging buffer into ctx->d_scratch and launch one CTA per job.
 // data: per job, N*N weights, P gammas, P betas (doubles, host); outputs go
@@ -99,13 +107,9 @@ static int run_small_jobs(fq_ctx* ctx, const SmallHostJob* jobs, int njobs, int 
     }
     FQ_CUDA(cudaMemcpyAsync(ctx->d_scratch, h, need, cudaMemcpyHostToDevice, ctx->stream));
     FQ_CUDA(cudaEventRecord(ctx->stage_evt, ctx->stream));
-    const size_t smem = small_smem_bytes(nmax);
-    FQ_CUDA(cudaFuncSetAttribute(k_small_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)small_smem_bytes(kSmallMaxQubits)));
     const int tok = prof_begin(ctx);
-    k_small_jobs<<<njobs, kSmallThreads, smem, ctx->stream>>>(
-        reinterpret_cast<const SmallJob*>(ctx->d_scratch), njobs);
-    FQ_CUDA(cudaGetLastError());
+    FQ_TRY(launch_small_jobs(reinterpret_cast<const SmallJob*>(ctx->d_scratch), njobs, nmax,
+                             ctx->stream));
     prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
     ctx->launches++;
     return FQ_OK;
@@ -126,35 +130,11 @@ static int check_angles(int P, const double* gammas, const double* betas) {
     return FQ_OK;
 }
 
-}  // namespace fq
-
-using namespace fq;
-
-extern "C" {
-
-int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, const double* graph,
-                        const double* gammas, const double* betas, double* energy,
-                        double* grad_gamma, double* grad_beta) {
-    FQ_TRY(validate_ctx(ctx));
-    FQ_CHECK(N >= 2 && N <= kMaxQubits, FQ_ERR_INVALID, "N=%d out of range [2,%d]", N,
-             kMaxQubits);
+// Enqueue the gradient of an N >= 13 circuit on ctx's stream; the results
+// land in ctx->h_result once the stream reaches this point (grad_collect).
+int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const double* graph,
+                 const double* gammas, const double* betas) {
     FQ_TRY(check_angles(P, gammas, betas));
-    FQ_CHECK(energy && grad_gamma && grad_beta, FQ_ERR_INVALID, "null output");
-    if (N <= kSmallMaxQubits) {
-        FQ_CHECK(1 + 2 * P <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
-        GraphPrep g;
-        FQ_TRY(prep_graph(graph, N, g));
-        SmallHostJob J{N, P, SJ_ENERGY | SJ_GRAD, g.wd.data(), gammas, betas, nullptr};
-        std::vector<int> off;
-        FQ_TRY(run_small_jobs(ctx, &J, 1, 0, off));
-        FQ_TRY(read_results(ctx, 1 + 2 * P));
-        *energy = ctx->h_result[0];
-        for (int k = 0; k < P; k++) {
-            grad_gamma[k] = ctx->h_result[1 + k];
-            grad_beta[k] = ctx->h_result[1 + P + k];
-        }
-        return FQ_OK;
-    }
     FQ_TRY(check_state(sv, N));
     FQ_TRY(check_state(costate, N));
     FQ_CHECK(sv != costate, FQ_ERR_INVALID, "state and costate must be different buffers");
@@ -162,7 +142,7 @@ int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, cons
     FQ_TRY(setup_graph(ctx, graph, N, g));
     const std::vector<PassPlan> plan = plan_layer(N);
     const int npass = (int)plan.size();
-    FQ_CHECK(1 + P + P * npass <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
+    FQ_CHECK(1 + P + P * npass < kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
 
     // Forward circuit, then lambda = C psi with <C>.
     FQ_TRY(engine_forward(ctx, sv, N, P, g, gammas, betas, nullptr));
@@ -203,8 +183,25 @@ int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, cons
             if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
         }
     }
-    FQ_TRY(read_results(ctx, 1 + P + P * npass));
+    FQ_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, sizeof(double) * (1 + P + P * npass),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    // The kernels' error flag travels with the results (last result word).
+    FQ_CUDA(cudaMemcpyAsync(ctx->h_result + kResultWords - 1, ctx->d_err, sizeof(int),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    return FQ_OK;
+}
+
+int grad_collect(fq_ctx* ctx, int N, int P, double* energy, double* grad_gamma,
+                 double* grad_beta) {
+    const int npass = (int)plan_layer(N).size();
     const double* r = ctx->h_result;
+    int flag = 0;
+    memcpy(&flag, r + kResultWords - 1, sizeof(int));
+    if (flag) {
+        FQ_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        set_error("a device-side bounded wait gave up (flag %d); results are incomplete", flag);
+        return FQ_ERR_TIMEOUT;
+    }
     *energy = r[0];
     for (int k = 0; k < P; k++) {
         grad_gamma[k] = -r[1 + k];
@@ -213,6 +210,40 @@ int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, cons
         grad_beta[k] = s;
     }
     return FQ_OK;
+}
+
+}  // namespace fq
+
+using namespace fq;
+
+extern "C" {
+
+int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, const double* graph,
+                        const double* gammas, const double* betas, double* energy,
+                        double* grad_gamma, double* grad_beta) {
+    FQ_TRY(validate_ctx(ctx));
+    FQ_CHECK(N >= 2 && N <= kMaxQubits, FQ_ERR_INVALID, "N=%d out of range [2,%d]", N,
+             kMaxQubits);
+    FQ_TRY(check_angles(P, gammas, betas));
+    FQ_CHECK(energy && grad_gamma && grad_beta, FQ_ERR_INVALID, "null output");
+    if (N <= kSmallMaxQubits) {
+        FQ_CHECK(1 + 2 * P <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
+        GraphPrep g;
+        FQ_TRY(prep_graph(graph, N, g));
+        SmallHostJob J{N, P, SJ_ENERGY | SJ_GRAD, g.wd.data(), gammas, betas, nullptr};
+        std::vector<int> off;
+        FQ_TRY(run_small_jobs(ctx, &J, 1, 0, off));
+        FQ_TRY(read_results(ctx, 1 + 2 * P));
+        *energy = ctx->h_result[0];
+        for (int k = 0; k < P; k++) {
+            grad_gamma[k] = ctx->h_result[1 + k];
+            grad_beta[k] = ctx->h_result[1 + P + k];
+        }
+        return FQ_OK;
+    }
+    FQ_TRY(grad_enqueue(ctx, sv, costate, N, P, graph, gammas, betas));
+    FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    return grad_collect(ctx, N, P, energy, grad_gamma, grad_beta);
 }
 
 }  // extern "C"

@@ -11,29 +11,9 @@
 // pow(1/sqrt(2), N)); the adjoint is the one of fq_pass_dual.cuh.
 #pragma once
 
-#include "fq_common.cuh"
+#include "fq_small.h"
 
 namespace fq {
-
-constexpr int kSmallMaxQubits = 12;
-constexpr int kSmallThreads = 256;
-
-enum { SJ_ENERGY = 1, SJ_GRAD = 2, SJ_STATE = 4 };
-
-struct SmallJob {
-    int N, P, flags, pad;
-    const double* w;       // N*N symmetric weights (device)
-    const double* gammas;  // P (device)
-    const double* betas;   // P (device)
-    double* out;           // [0] <C>, [1..P] dE/dgamma, [1+P..2P] dE/dbeta (device)
-    double2* state;        // final forward state (SJ_STATE), 2^N (device)
-};
-
-__host__ __device__ inline size_t small_smem_bytes(int nmax) {
-    const size_t n = (size_t)1 << nmax;
-    return 2 * n * sizeof(double2) + n * sizeof(double) +
-           sizeof(double) * (kSmallMaxQubits * kSmallMaxQubits + kSmallThreads);
-}
 
 // Fixed-order block sum (same bits for the same inputs).
 __device__ __forceinline__ double small_block_sum(double v, double* sh) {

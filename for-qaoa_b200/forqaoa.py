@@ -64,7 +64,33 @@ SIGNATURES = {
     "fq_permute_qubits": (_i, [_vp, _vp, _vp, _i, _ip]),
     "fq_reference_label_map": (_i, [_i, _i, _i, _ip]),
     "fq_expectation_noalloc": (_i, [_vp, _i, _dp, _dp, _vp]),
+    "fq_server_create": (_i, [_i, _d, _i, ctypes.POINTER(_vp)]),
+    "fq_server_destroy": (_i, [_vp]),
+    "fq_server_submit": (_i, [_vp, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "fq_server_poll": (_i, [_vp, ctypes.c_void_p, _i, _ip, _i]),
+    "fq_server_close_session": (_i, [_vp, ctypes.c_uint64]),
+    "fq_server_stats": (_i, [_vp, ctypes.c_void_p]),
 }
+
+SERVE_MAX_LAYERS = 16  # FQ_SERVE_MAX_LAYERS
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("session", ctypes.c_uint64), ("N", _i), ("P", _i), ("graph_upper", _dp),
+                ("gammas", _dp), ("betas", _dp)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("session", ctypes.c_uint64), ("N", _i),
+                ("P", _i), ("status", _i), ("pad", _i), ("energy", _d),
+                ("grad_gamma", _d * SERVE_MAX_LAYERS), ("grad_beta", _d * SERVE_MAX_LAYERS),
+                ("t_submit", _d), ("t_start", _d), ("t_done", _d)]
+
+
+class _Counters(ctypes.Structure):
+    _fields_ = [("pending", ctypes.c_longlong), ("kernel_launches", ctypes.c_longlong),
+                ("batched_requests", ctypes.c_longlong), ("lane_requests", ctypes.c_longlong),
+                ("resident_sessions", ctypes.c_longlong), ("resident_bytes", _d)]
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(_lib, _name)
     _f.restype = _res
@@ -317,3 +343,97 @@ class Context:
                     _check(_lib.fq_relabel_graph(_dptr(g), n, 0, swap_in, sizes[i + 1]),
                            "fq_relabel_graph")
         return g
+
+
+class ServeResult:
+    """One finished request of a Server."""
+    __slots__ = ("ticket", "session", "N", "P", "status", "energy", "grad_gamma", "grad_beta",
+                 "t_submit", "t_start", "t_done")
+
+    def __init__(self, r):
+        self.ticket, self.session = int(r.ticket), int(r.session)
+        self.N, self.P, self.status = r.N, r.P, r.status
+        self.energy = r.energy
+        self.grad_gamma = np.array(r.grad_gamma[:r.P])
+        self.grad_beta = np.array(r.grad_beta[:r.P])
+        self.t_submit, self.t_start, self.t_done = r.t_submit, r.t_start, r.t_done
+
+    @property
+    def latency(self):
+        return self.t_done - self.t_submit
+
+
+class Server:
+    """Continuous batching of energy+gradient requests on one device
+    (fq_server_* in include/forqaoa.h).  submit() returns a ticket; poll()
+    returns finished ServeResults in completion order."""
+
+    def __init__(self, device=0, hbm_budget_bytes=150e9, lanes=4):
+        h = _vp()
+        _check(_lib.fq_server_create(device, float(hbm_budget_bytes), lanes, ctypes.byref(h)),
+               "fq_server_create")
+        self.handle = h
+        self._stash = []  # results polled by wait() for other tickets
+
+    def close(self):
+        if self.handle:
+            _check(_lib.fq_server_destroy(self.handle), "fq_server_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, session, graph, gammas, betas):
+        g, ga, be = _f64(graph), _f64(gammas), _f64(betas)
+        assert ga.shape == be.shape and g.shape[0] == g.shape[1]
+        q = _Request(session, g.shape[0], len(ga), _dptr(g), _dptr(ga), _dptr(be))
+        t = ctypes.c_uint64()
+        _check(_lib.fq_server_submit(self.handle, ctypes.byref(q), ctypes.byref(t)),
+               "fq_server_submit")
+        return int(t.value)
+
+    def _poll_lib(self, max_results, wait_ms):
+        buf = (_Result * max_results)()
+        n = _i()
+        _check(_lib.fq_server_poll(self.handle, buf, max_results, ctypes.byref(n), wait_ms),
+               "fq_server_poll")
+        return [ServeResult(buf[i]) for i in range(n.value)]
+
+    def poll(self, max_results=1024, wait_ms=0):
+        if self._stash:
+            out, self._stash = self._stash[:max_results], self._stash[max_results:]
+            return out
+        return self._poll_lib(max_results, wait_ms)
+
+    def wait(self, tickets, timeout_s=600.0):
+        """Polls until every ticket in `tickets` is done; returns {ticket: result}.
+        Results of other tickets stay queued for poll()."""
+        import time
+        want, got, keep = set(tickets), {}, []
+        for r in self._stash:
+            if r.ticket in want:
+                got[r.ticket] = r
+            else:
+                keep.append(r)
+        self._stash = keep
+        t_end = time.monotonic() + timeout_s
+        while want - got.keys():
+            if time.monotonic() > t_end:
+                raise TimeoutError(f"{len(want - got.keys())} requests not done")
+            for r in self._poll_lib(1024, 50):
+                if r.ticket in want:
+                    got[r.ticket] = r
+                else:
+                    self._stash.append(r)
+        return got
+
+    def close_session(self, session):
+        _check(_lib.fq_server_close_session(self.handle, session), "fq_server_close_session")
+
+    def stats(self):
+        c = _Counters()
+        _check(_lib.fq_server_stats(self.handle, ctypes.byref(c)), "fq_server_stats")
+        return {k: getattr(c, k) for k, _ in _Counters._fields_}

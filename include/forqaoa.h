@@ -165,6 +165,64 @@ int fq_expectation_noalloc(const void* sv, int N, const double* graph_upper, dou
  * at physical position b.  Host only. */
 int fq_reference_label_map(int N, int C, int P, int* label_map);
 
+/* ---- serving -------------------------------------------------------------
+ * A server admits energy+gradient requests (fq_qaoa_energy_grad's
+ * computation) and runs them with continuous batching on one device:
+ * requests with N <= 12 are packed one per CTA into batched launches,
+ * larger ones overlap on `lanes` independent streams.  Requests of one
+ * session (an optimiser loop on one graph) run in submission order and, for
+ * N >= 13, keep their state and costate buffers (2 x 16 x 2^N bytes)
+ * resident between steps; resident buffers stay within hbm_budget_bytes,
+ * idle sessions being released least recently used first.  No counterpart
+ * in the reference, whose CLI runs one circuit per process
+ * (src/Weighted.cpp:58-160). */
+#define FQ_SERVE_MAX_LAYERS 16
+
+typedef struct fq_server fq_server;
+
+typedef struct fq_request {
+    uint64_t session;           /* caller's session id */
+    int N, P;                   /* 2 <= N <= 33, 1 <= P <= FQ_SERVE_MAX_LAYERS */
+    const double* graph_upper;  /* N*N row-major, upper triangle read; copied */
+    const double* gammas;       /* P; copied */
+    const double* betas;        /* P; copied */
+} fq_request;
+
+typedef struct fq_result {
+    uint64_t ticket, session;
+    int N, P, status, pad;
+    double energy;
+    double grad_gamma[FQ_SERVE_MAX_LAYERS];
+    double grad_beta[FQ_SERVE_MAX_LAYERS];
+    double t_submit, t_start, t_done; /* steady clock, seconds */
+} fq_result;
+
+typedef struct fq_server_counters {
+    long long pending;           /* submitted, not yet polled as done */
+    long long kernel_launches;   /* kernels launched so far */
+    long long batched_requests;  /* requests run in one-CTA batches */
+    long long lane_requests;     /* requests run on lanes */
+    long long resident_sessions; /* sessions holding device buffers */
+    double resident_bytes;       /* their bytes */
+} fq_server_counters;
+
+/* Starts a server with its scheduler thread on `device`. */
+int fq_server_create(int device, double hbm_budget_bytes, int lanes, fq_server** out);
+/* Finishes every submitted request, then frees everything. */
+int fq_server_destroy(fq_server* server);
+/* Queues a request (validated and copied); *ticket identifies its result.
+ * FQ_ERR_OOM if one session of this N exceeds the budget. */
+int fq_server_submit(fq_server* server, const fq_request* request, uint64_t* ticket);
+/* Moves up to max_results finished results to out (completion order),
+ * waiting up to wait_ms for the first; *n_out = number moved.  A non-OK
+ * return reports the first failure the scheduler met (per-request status is
+ * in each result). */
+int fq_server_poll(fq_server* server, fq_result* out, int max_results, int* n_out,
+                   int wait_ms);
+/* Releases a session's resident buffers (after its running step, if any). */
+int fq_server_close_session(fq_server* server, uint64_t session);
+int fq_server_stats(fq_server* server, fq_server_counters* counters);
+
 #ifdef __cplusplus
 }
 #endif
