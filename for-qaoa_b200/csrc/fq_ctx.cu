@@ -72,6 +72,13 @@ int prep_graph(const double* upper, int N, GraphPrep& g) {
             }
         }
     g.W = W;
+    g.gmax = 0;
+    if (integral)
+        for (int u = 0; u < N; u++) {
+            long long d = 0;
+            for (int v = 0; v < N; v++) d += g.wi[u * N + v] > 0 ? g.wi[u * N + v] : -g.wi[u * N + v];
+            g.gmax = std::max(g.gmax, d);
+        }
     g.integer = integral && absum < (1ll << 30) && (pos - neg + 1) <= kMaxPhaseTable;
     g.W_int = pos + neg;
     g.cmin = neg;

@@ -57,6 +57,7 @@ struct GraphPrep {
     long long W_int = 0;       // sum of weights (integer path)
     double W = 0;              // sum of weights
     long long cmin = 0, cmax = 0;  // range of cut values (integer path)
+    long long gmax = 0;            // max over qubits of sum_v |w_uv| (integer path)
 };
 
 int prep_graph(const double* upper, int N, GraphPrep& g);

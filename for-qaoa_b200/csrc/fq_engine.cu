@@ -29,19 +29,17 @@ __global__ void k_phase_table(double2* tab, int cmin, int n, long long W, double
     }
 }
 
-// Two-level phase table of the engine: tab[j] = exp(i*gamma*j) for j < 32,
-// tab[32 + h] = scale * (cos, sin)(S * gamma / 2) with S = 2(cmin + 32h) - W.
-__global__ void k_phase_table2(double2* tab, int cmin, int nhi, long long W, double gamma,
-                               double scale) {
+// Two-level table of powers of z = exp(i*gamma) used by the engine's
+// passes: tab[j] = z^j for j < 32, tab[32 + h] = z^(dlo + 32h).
+__global__ void k_phase_table2(double2* tab, int dlo, int nhi, double gamma) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double sn, cs;
     if (i < kPhaseLo) {
         sincos(gamma * (double)i, &sn, &cs);
         tab[i] = make_double2(cs, sn);
     } else if (i < kPhaseLo + nhi) {
-        const double S = (double)(2ll * (cmin + 32ll * (i - kPhaseLo)) - W);
-        sincos(S * gamma / 2, &sn, &cs);
-        tab[i] = make_double2(cs * scale, sn * scale);
+        sincos(gamma * (double)(dlo + 32ll * (i - kPhaseLo)), &sn, &cs);
+        tab[i] = make_double2(cs, sn);
     }
 }
 
@@ -230,25 +228,47 @@ PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     return A;
 }
 
-// High-part entries of the engine's two-level phase table (0: the range is
-// too wide for shared memory and the one-level global table is used).
+// Range [dlo, dhi] of the powers of z the passes look up: every cut value
+// and every single-qubit flip change g (|g| <= gmax).
+static void table_range(const GraphPrep& g, long long& dlo, long long& dhi) {
+    dlo = std::min(g.cmin, -g.gmax);
+    dhi = std::max(g.cmax, g.gmax);
+}
+
+// High-part entries of the engine's two-level table (0: the range is too
+// wide for shared memory and the one-level global phase table is used).
 int engine_nhi(const GraphPrep& g) {
-    const long long range = g.cmax - g.cmin + 1;
-    const long long nhi = (range + kPhaseLo - 1) / kPhaseLo;
+    long long dlo, dhi;
+    table_range(g, dlo, dhi);
+    const long long nhi = (dhi - dlo + 1 + kPhaseLo - 1) / kPhaseLo;
     return nhi <= kPhaseHiMax ? (int)nhi : 0;
 }
 
-int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
+int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma) {
     const int nhi = engine_nhi(g);
     if (nhi == 0) return FQ_ERR_INVALID;
+    long long dlo, dhi;
+    table_range(g, dlo, dhi);
     const int n = kPhaseLo + nhi;
     const int tok = prof_begin(ctx);
-    k_phase_table2<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ptab, (int)g.cmin, nhi,
-                                                              g.W_int, gamma, scale);
+    k_phase_table2<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->d_ptab, (int)dlo, nhi, gamma);
     FQ_CUDA(cudaGetLastError());
     prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
     ctx->launches++;
     return FQ_OK;
+}
+
+void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale) {
+    A.nhi = engine_nhi(g);
+    if (A.nhi > 0) {
+        long long dlo, dhi;
+        table_range(g, dlo, dhi);
+        A.dlo = (int)dlo;
+        A.ntab = (int)(dhi - dlo + 1);
+        const double th = -gamma * (double)g.W_int / 2;
+        A.ph0x = scale * cos(th);
+        A.ph0y = scale * sin(th);
+    }
 }
 
 int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale) {
@@ -315,7 +335,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
         const int nhi = g.integer ? engine_nhi(g) : 0;
         if (g.integer) {
             if (nhi > 0)
-                FQ_TRY(launch_table2(ctx, g, gammas[p], scale));
+                FQ_TRY(launch_table2(ctx, g, gammas[p]));
             else
                 FQ_TRY(launch_table(ctx, g, gammas[p], scale));
         }
@@ -325,7 +345,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
             A.a = plan[i].a;
             A.tmask = plan[i].tmask;
             A.gx = gx;
-            A.nhi = nhi;
+            if (nhi > 0) set_table_args(A, g, gammas[p], scale);
             A.gamma = gammas[p];
             A.scale = g.integer ? 1.0 : scale;
             const int ph = i == 0 ? (p == 0 ? PH_INIT : PH_MUL) : PH_NONE;

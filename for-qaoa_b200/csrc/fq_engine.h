@@ -25,7 +25,10 @@ void gate_params(double beta, int& gm, double& g, double& f);
 PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g);
 // High-part entries of the two-level phase table (0: use the global table).
 int engine_nhi(const GraphPrep& g);
-int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
+// Two-level table of powers of exp(i*gamma) in ctx->d_ptab (nhi > 0), and
+// the pass arguments that read it (nhi, dlo, ntab, ph0 = scale*exp(-i*gamma*W/2)).
+int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma);
+void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale);
 int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
 // Fixed-order sum of n partials into one device word.
 int reduce_partials(fq_ctx* ctx, const double* partial, int n, double* out_dev);

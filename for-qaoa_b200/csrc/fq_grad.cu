@@ -160,7 +160,7 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
         const int nhi = g.integer ? engine_nhi(g) : 0;
         if (g.integer) {
             if (nhi > 0)
-                FQ_TRY(launch_table2(ctx, g, gammas[k], 1.0));
+                FQ_TRY(launch_table2(ctx, g, gammas[k]));
             else
                 FQ_TRY(launch_table(ctx, g, gammas[k], 1.0));
         }
@@ -174,7 +174,7 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             A.c = cos(betas[k] / 2);
             A.s = -sin(betas[k] / 2);  // RX(-beta)
             A.gamma = gammas[k];
-            A.nhi = nhi;
+            if (nhi > 0) set_table_args(A, g, gammas[k], 1.0);
             A.scale = k > 0 ? 1.0 : 0.0;  // inverse phase only where layers remain
             const int grid = (int)std::min<i64>(A.ntiles, ctx->num_sms);
             double* gg = gb + grid;

@@ -72,16 +72,19 @@ struct PassArgs {
     double2* sv2;         // second vector: costate output (EX_COSTATE)
     const void* w;        // N*N symmetric weights (int32 or float64), device
     // Integer path: the phase of cut value c.  nhi == 0: one table in global
-    // memory, ptab[c - cmin].  nhi > 0: two small tables copied to shared
-    // memory, ptab[0..32) = exp(i*gamma*j) and ptab[32 + h] = phase of
-    // cmin + 32h, so phase(c) = hi[(c - cmin) >> 5] * lo[(c - cmin) & 31].
+    // memory, ptab[c - cmin] = scale * exp(i*gamma*(2c - W)/2).  nhi > 0:
+    // powers of z = exp(i*gamma) in two small tables copied to shared
+    // memory, ptab[j] = z^j (j < 32) and ptab[32 + h] = z^(dlo + 32h), so
+    // z^d = hi[(d - dlo) >> 5] * lo[(d - dlo) & 31] for d in [dlo, dlo + ntab)
+    // and phase(c) = ph0 * z^c with ph0 = scale * exp(-i*gamma*W/2).
     const double2* ptab;
     double* partial;      // <C> partial sums, one per CTA
     double* diag;         // cut-value output (EX_DIAG)
     i64 ntiles;
     int N, l, a;
     unsigned tmask;  // RX targets among the 12 tile bits
-    int cmin, ntab, nhi;
+    int cmin, ntab, nhi, dlo;
+    double ph0x, ph0y;  // ph0 of the two-level table (see ptab)
     double gx;       // t or u of the reduced gate
     double c, s;     // cos, sin of angle/2 for GM_FULL
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
@@ -108,13 +111,20 @@ __device__ __forceinline__ void load_phase_tables(const PassArgs& A, double2* sm
         for (int i = tid; i < kPhaseLo + A.nhi; i += nthreads) smtab[i] = A.ptab[i];
 }
 
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// z^d from the two-level table in shared memory (nhi > 0).
+__device__ __forceinline__ double2 tab_pow(const PassArgs& A, const double2* smtab, int d) {
+    const int ti = min(max(d - A.dlo, 0), A.ntab - 1);  // guards the table read only
+    return cmul(smtab[kPhaseLo + (ti >> 5)], smtab[ti & 31]);
+}
+
 // Phase (times the layer's scale) of a cut value on the integer path.
 __device__ __forceinline__ double2 int_phase(const PassArgs& A, const double2* smtab, int cr) {
+    if (A.nhi > 0) return cmul(make_double2(A.ph0x, A.ph0y), tab_pow(A, smtab, cr));
     const int ti = min(max(cr - A.cmin, 0), A.ntab - 1);  // guards the table read only
-    if (A.nhi > 0) {
-        const double2 h = smtab[kPhaseLo + (ti >> 5)], lo = smtab[ti & 31];
-        return make_double2(h.x * lo.x - h.y * lo.y, h.x * lo.y + h.y * lo.x);
-    }
     return __ldg(A.ptab + ti);
 }
 
@@ -207,8 +217,9 @@ __device__ __forceinline__ void exchange_g(double2 (&v)[kRegs], double2* buf, in
 }
 
 template <int LF, int LT>
-__device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid) {
-    __syncthreads();  // previous readers of buf are done
+__device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid,
+                                         bool wait_readers = true) {
+    if (wait_readers) __syncthreads();  // previous readers of buf are done
 #pragma unroll
     for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
     __syncthreads();
@@ -216,60 +227,120 @@ __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int 
     for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
 }
 
-// Shared-memory bytes a pass needs for N qubits and weight type WT.
+constexpr int kWfStride = 21;  // row stride of the compact weight tables (odd: no bank conflicts)
+static_assert(kWfStride >= kMaxFixed, "compact weight rows hold every fixed bit");
+
+// Physical bit of fixed (non-tile) index i, ascending.
+__device__ __forceinline__ int fixed_phys(int i, int l, int a) {
+    const int nmid = a - l;
+    return i < nmid ? l + i : a + (kTileBits - l) + (i - nmid);
+}
+
+// Offset of tile index t (12 bits) from the tile's base amplitude.
+__device__ __forceinline__ i64 tile_off(int t, int l, int a) {
+    return (i64)(t & ((1 << l) - 1)) | ((i64)(t >> l) << a);
+}
+
+// Shared-memory layout of k_pass after the 64 KB exchange buffer (which
+// also holds the N*N weights while the kernel sets up).
 template <typename WT>
-__host__ __device__ inline size_t pass_smem_bytes(int N) {
-    return sizeof(double2) * kTile + sizeof(double) * 8 + sizeof(i64) * 32 + sizeof(int) * 24 +
-           sizeof(WT) * (N * N + 32 + 16 + 24 + 16) + 16 + phase_smem_bytes();
+struct PassSmem {
+    static constexpr size_t red = 0;                                // 8 double
+    static constexpr size_t ke = red + 8 * sizeof(double);          // 2 x 32 WT
+    static constexpr size_t creg = ke + 64 * sizeof(WT);            // 16 WT
+    static constexpr size_t Dm = creg + 16 * sizeof(WT);            // 24 WT
+    static constexpr size_t Ru = Dm + 24 * sizeof(WT);              // 16 WT
+    static constexpr size_t wf = Ru + 16 * sizeof(WT);              // kMaxFixed x kWfStride
+    static constexpr size_t wu = wf + kMaxFixed * kWfStride * sizeof(WT);  // 12 x kWfStride
+    static constexpr size_t thrc = wu + kTileBits * kWfStride * sizeof(WT);  // 5 x 256 WT
+    static constexpr size_t qtab = (thrc + 5 * kPassThreads * sizeof(WT) + 15) & ~(size_t)15;
+    static constexpr size_t smtab = qtab + 16 * sizeof(double2);
+    static constexpr size_t bytes = smtab + sizeof(double2) * (kPhaseLo + kPhaseHiMax);
+};
+
+// Shared-memory bytes k_pass needs (independent of N: the weights are
+// staged in the exchange buffer).
+template <typename WT>
+__host__ __device__ inline size_t pass_smem_bytes(int) {
+    return sizeof(double2) * kTile + PassSmem<WT>::bytes;
+}
+
+// Cut value of register slot r: c_r = cbase + creg[r] + sum_k r_k g_k, so
+// its phase factors as phase(c_r) = P * Q_r * prod_k E_k^(r_k) with
+// P = phase(cbase), Q_r = z^creg[r] (per pass, shared memory) and
+// E_k = z^g_k, z = exp(i*gamma): 5 table lookups (or sincos) per thread and
+// tile instead of 16.  Applied in stages to keep few values live: first
+// P * Q_r on every slot (PH_INIT writes it, PH_MUL multiplies it in,
+// src/rzz.cu:153-154), then E_k on the slots with bit k set.
+template <int PH>
+__device__ __forceinline__ void phase_base(double2 (&v)[kRegs], double2 P, const double2* qtab) {
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) {
+        const double2 ph = cmul(P, qtab[r]);
+        v[r] = (PH == PH_INIT) ? ph : cmul(v[r], ph);
+    }
+}
+
+__device__ __forceinline__ void phase_bit(double2 (&v)[kRegs], int k, double2 E) {
+#pragma unroll
+    for (int r = 0; r < kRegs; r++)
+        if ((r >> k) & 1) v[r] = cmul(v[r], E);
 }
 
 template <typename WT, int PH, int GM, int EX, bool ST, int SC>
 __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    using SM = PassSmem<WT>;
     double2* buf = reinterpret_cast<double2*>(smraw);
+    unsigned char* const sm = smraw + sizeof(double2) * kTile;
+    double* red = reinterpret_cast<double*>(sm + SM::red);
+    WT* ke = reinterpret_cast<WT*>(sm + SM::ke);      // 2 x 32: [0] = K, [1+u] = e_u
+    WT* creg = reinterpret_cast<WT*>(sm + SM::creg);  // cut among the register bits
+    WT* Dm = reinterpret_cast<WT*>(sm + SM::Dm);
+    WT* Ru = reinterpret_cast<WT*>(sm + SM::Ru);
+    WT* wf = reinterpret_cast<WT*>(sm + SM::wf);      // wf[i][j] = w(fixed i, fixed j)
+    WT* wu = reinterpret_cast<WT*>(sm + SM::wu);      // wu[u][j] = w(tile u, fixed j)
+    WT* thrc = reinterpret_cast<WT*>(sm + SM::thrc);  // per-thread cut constants
+    double2* qtab = reinterpret_cast<double2*>(sm + SM::qtab);
+    double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
-    double* red = reinterpret_cast<double*>(buf + kTile);  // 8 warp partials
-    i64* offtab = reinterpret_cast<i64*>(red + 8);          // register-slot offsets: L0, L1
-    int* fpos = reinterpret_cast<int*>(offtab + 32);        // nF fixed positions, ascending
-    WT* sw = reinterpret_cast<WT*>(fpos + 24);             // N*N weights
-    WT* ke = sw + N * N;                                   // [0] = K, [1+u] = e_u
-    WT* creg = ke + 32;                                    // 16: cut among register bits
-    WT* Dm = creg + 16;                                    // nF
-    WT* Ru = Dm + 24;                                      // 12
-    double2* smtab = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);  // phase tables
     constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
     constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
     constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
+    constexpr bool INTW = sizeof(WT) == sizeof(int);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
+    // Product-tree phases: FP64 weights always, integer weights with the
+    // two-level table (nhi == 0 keeps one global-table lookup per amplitude).
+    const bool tree = PH != PH_NONE && (!INTW || A.nhi > 0);
 
-    if (tid < 2 * kRegs) {
-        // Offset of register slot r: tile bits 8..11 in L0, 4..7 in L1.
-        const int r = tid & 15, lo = tid < kRegs ? 8 : 4;
-        i64 o = 0;
-        for (int k = 0; k < 4; k++)
-            if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
-        offtab[tid] = o;
-    }
+    // ---- set-up: compact weight tables of this pass's tile geometry
+    WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
     if (CUT) {
         const WT* gw = reinterpret_cast<const WT*>(A.w);
         for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
-        if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
     }
-    if (PH != PH_NONE && sizeof(WT) == sizeof(int)) load_phase_tables(A, smtab, tid, kPassThreads);
+    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, tid, kPassThreads);
     __syncthreads();
     if (CUT) {
+        for (int idx = tid; idx < nF * nF; idx += kPassThreads) {
+            const int i = idx / nF, j = idx - i * nF;
+            wf[i * kWfStride + j] = sw[fixed_phys(i, l, a) * N + fixed_phys(j, l, a)];
+        }
+        for (int idx = tid; idx < kTileBits * nF; idx += kPassThreads) {
+            const int u = idx / nF, j = idx - u * nF;
+            wu[u * kWfStride + j] = sw[tile_phys(u, l, a) * N + fixed_phys(j, l, a)];
+        }
         if (tid < nF) {
-            const int m = fpos[tid];
+            const int m = fixed_phys(tid, l, a);
             WT d = 0;
             for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
             Dm[tid] = d;
         } else if (tid >= 32 && tid < 32 + kTileBits) {
             const int u = tile_phys(tid - 32, l, a);
             WT r = 0;
-            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
+            for (int i = 0; i < nF; i++) r += sw[u * N + fixed_phys(i, l, a)];
             Ru[tid - 32] = r;
         } else if (tid >= 64 && tid < 80) {
             const int r = tid - 64;
@@ -279,11 +350,16 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                     if (((r >> k) ^ (r >> k2)) & 1)
                         c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
             creg[r] = c;
+            if (PH != PH_NONE) {
+                double sn, cs;
+                sincos(A.gamma * (double)c, &sn, &cs);
+                qtab[r] = make_double2(cs, sn);
+            }
         }
-    }
-    // Per-thread constants of the cut decomposition (layout L0).
-    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
-    if (CUT) {
+        // Per-thread constants of the cut decomposition (layout L0), kept in
+        // shared memory: thrc[0] = cut among the thread's 8 tile bits plus
+        // their edges to set register bits, thrc[1+k] = f_k.
+        WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
         for (int j = 0; j < 8; j++) {
             const int pj = tile_phys(j, l, a);
             const int tj = (tid >> j) & 1;
@@ -305,15 +381,28 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 f3 += w3;
             }
         }
+        thrc[tid] = athr;
+        thrc[kPassThreads + tid] = f0;
+        thrc[2 * kPassThreads + tid] = f1;
+        thrc[3 * kPassThreads + tid] = f2;
+        thrc[4 * kPassThreads + tid] = f3;
     }
-    // Address pieces: thread part and the 4 register-bit strides (layout L0).
-    i64 thr_off = 0, thr_off1 = 0;
-    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    {
-        const int t1 = lay_index<1>(tid, 0);
-        for (int j = 0; j < kTileBits; j++)
-            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
-    }
+    __syncthreads();  // the weights in buf are dead from here on
+
+    // Address pieces: the thread's offsets in layouts L0 and L1 and the
+    // strides of the 4 register bits of each (uniform across the grid).
+    const i64 thr_off = tile_off(tid, l, a);
+    const i64 thr_off1 = tile_off(lay_index<1>(tid, 0), l, a);
+    const i64 s8 = 1ll << tile_phys(8, l, a), s9 = 1ll << tile_phys(9, l, a);
+    const i64 s10 = 1ll << tile_phys(10, l, a), s11 = 1ll << tile_phys(11, l, a);
+    const i64 s4 = 1ll << tile_phys(4, l, a), s5 = 1ll << tile_phys(5, l, a);
+    const i64 s6 = 1ll << tile_phys(6, l, a), s7 = 1ll << tile_phys(7, l, a);
+    auto off0 = [&](int r) -> i64 {
+        return ((r & 1) ? s8 : 0) + ((r & 2) ? s9 : 0) + ((r & 4) ? s10 : 0) + ((r & 8) ? s11 : 0);
+    };
+    auto off1 = [&](int r) -> i64 {
+        return ((r & 1) ? s4 : 0) + ((r & 2) ? s5 : 0) + ((r & 4) ? s6 : 0) + ((r & 8) ? s7 : 0);
+    };
     const int pf_step = l < 3 ? l : 3;  // prefetch granularity: 128-byte lines or rows
     const bool contiguous = (l == kTileBits);
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
@@ -322,11 +411,20 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double acc = 0, comp = 0;  // Kahan-compensated <C> accumulator
 
-    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x) {
+    int par = 0;
+    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
         const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        double2* const p = A.sv + base + thr_off;
+        double2 v[kRegs];
+        // The loads go out first; the tile's cut constants are computed
+        // while they are in flight.
+#pragma unroll
+        for (int r = 0; r < kRegs; r++) {
+            if (LOAD) v[r] = __ldcs(p + off0(r));
+            else v[r] = make_double2(0.0, 0.0);
+        }
         if (LOAD && A.pf_dist > 0) {
-            // Stream this CTA's tile pf_dist strides ahead from HBM into L2
-            // while the current one is computed: the loads below then hit L2.
+            // Stream this CTA's tile pf_dist strides ahead from HBM into L2.
             const i64 T2 = T + (i64)A.pf_dist * gridDim.x;
             if (T2 < A.ntiles) {
                 const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
@@ -339,81 +437,88 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 } else {
                     for (int j = tid; j < (1 << (kTileBits - pf_step)); j += kPassThreads) {
                         const int t = j << pf_step;
-                        const i64 off = (i64)(t & ((1 << l) - 1)) | ((i64)(t >> l) << a);
-                        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + b2 + off) : "memory");
+                        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + b2 + tile_off(t, l, a))
+                                     : "memory");
                     }
                 }
             }
         }
-        if (CUT) {
-            __syncthreads();  // previous tile's readers of ke are done
-            if (warp == 0) {
-                WT h = 0;
-                if (lane < nF) {
-                    const int m = fpos[lane];
-                    const int zm = (int)((base >> m) & 1);
-                    if (zm) h += Dm[lane];
-                    for (int i = lane + 1; i < nF; i++)
-                        if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-                WT e = 0;
-                if (lane < kTileBits) {
-                    const int u = tile_phys(lane, l, a);
-                    e = Ru[lane];
-                    for (int i = 0; i < nF; i++)
-                        if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
-                    ke[1 + lane] = e;
-                }
-                if (lane == 0) ke[0] = h;
-            }
-            __syncthreads();
-        }
-        double2* const p = A.sv + base + thr_off;
-        double2 v[kRegs];
-        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
-        if (CUT) {
-            cbase = ke[0] + athr;
+        // cbase = cut value of the thread's slot 0, g_k = change when register
+        // bit k is set (from this tile's K, e_u and the thread's constants).
+        WT* const kp = ke + 32 * par;
+        auto cut_consts = [&](WT& cb, WT& h0, WT& h1, WT& h2, WT& h3) {
+            cb = kp[0] + thrc[tid];
 #pragma unroll
             for (int j = 0; j < 8; j++)
-                if ((tid >> j) & 1) cbase += ke[1 + j];
-            g0 = f0 + ke[9];
-            g1 = f1 + ke[10];
-            g2 = f2 + ke[11];
-            g3 = f3 + ke[12];
-        }
+                if ((tid >> j) & 1) cb += kp[1 + j];
+            h0 = thrc[kPassThreads + tid] + kp[9];
+            h1 = thrc[2 * kPassThreads + tid] + kp[10];
+            h2 = thrc[3 * kPassThreads + tid] + kp[11];
+            h3 = thrc[4 * kPassThreads + tid] + kp[12];
+        };
+        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+        if (CUT) {
+            // K and e_u of this tile (warps 0 and 1), double-buffered so the
+            // previous tile's readers need no barrier of their own.
+            if (warp < 2) {
+                const int zi = lane < nF ? (int)((base >> fixed_phys(lane, l, a)) & 1) : 0;
+                const unsigned F = __ballot_sync(0xffffffffu, zi);
+                if (warp == 0) {
+                    WT h = 0;
+                    if (lane < nF) {
+                        if (zi) h = Dm[lane];
+                        const WT* row = wf + lane * kWfStride;
 #pragma unroll
-        for (int r = 0; r < kRegs; r++) {
-            if (LOAD) v[r] = __ldcs(p + offtab[r]);
-            else v[r] = make_double2(0.0, 0.0);
+                        for (int j = 1; j < kMaxFixed; j++)
+                            if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi))
+                                h += row[j];
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+                    if (lane == 0) kp[0] = h;
+                } else if (lane < kTileBits) {
+                    WT e = Ru[lane];
+                    const WT* row = wu + lane * kWfStride;
+#pragma unroll
+                    for (int j = 0; j < kMaxFixed; j++)
+                        if (j < nF && ((F >> j) & 1u)) e -= 2 * row[j];
+                    kp[1 + lane] = e;
+                }
+            }
+            __syncthreads();
+            cut_consts(cbase, g0, g1, g2, g3);
         }
         if (PH != PH_NONE) {
-#pragma unroll
-            for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
-                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
-                double2 ph;
-                if (sizeof(WT) == sizeof(int)) {
-                    ph = int_phase(A, smtab, (int)cr);
-                } else {
-                    const double S = 2.0 * (double)cr - A.W;
+            if (tree) {
+                auto zpow = [&](WT d) -> double2 {  // z^d
+                    if (INTW) return tab_pow(A, smtab, (int)d);
                     double sn, cs;
-                    sincos(S * A.gamma / 2, &sn, &cs);
-                    ph.x = cs;
-                    ph.y = sn;
-                }
-                if (PH == PH_INIT) {
-                    v[r].x = ph.x * A.scale;
-                    v[r].y = ph.y * A.scale;
+                    sincos(A.gamma * (double)d, &sn, &cs);
+                    return make_double2(cs, sn);
+                };
+                double2 P;
+                if (INTW) {
+                    P = cmul(make_double2(A.ph0x, A.ph0y), tab_pow(A, smtab, (int)cbase));
+                    if (PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
                 } else {
-                    if (sizeof(WT) != sizeof(int)) {
-                        ph.x *= A.scale;
-                        ph.y *= A.scale;
-                    }
-                    const double2 in = v[r];
-                    v[r].x = in.x * ph.x - in.y * ph.y;  // src/rzz.cu:153-154
-                    v[r].y = in.x * ph.y + in.y * ph.x;
+                    double sn, cs;
+                    sincos(A.gamma * ((double)cbase - 0.5 * A.W), &sn, &cs);
+                    P = make_double2(cs * A.scale, sn * A.scale);
+                }
+                phase_base<PH>(v, P, qtab);
+                phase_bit(v, 0, zpow(g0));
+                phase_bit(v, 1, zpow(g1));
+                phase_bit(v, 2, zpow(g2));
+                phase_bit(v, 3, zpow(g3));
+            } else {
+#pragma unroll
+                for (int r = 0; r < kRegs; r++) {
+                    const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) +
+                                  ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
+                                  ((r & 8) ? g3 : WT(0));
+                    const double2 ph = int_phase(A, smtab, (int)cr);
+                    v[r] = (PH == PH_INIT) ? make_double2(ph.x * A.scale, ph.y * A.scale)
+                                           : cmul(v[r], ph);
                 }
             }
         }
@@ -423,24 +528,29 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         if (GM != GM_NONE) {
             rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
             if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
+            // With the cut barrier above, every thread is past the previous
+            // tile's reads of buf: the first exchange needs no barrier first.
             if (SC == SC_L021) {
-                exchange<0, 2>(v, buf, tid);
+                exchange<0, 2>(v, buf, tid, !CUT);
                 rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
-                exchange<2, 1>(v, buf, tid);
+                exchange<2, 1>(v, buf, tid, true);
             } else if (SC == SC_L01) {
-                exchange<0, 1>(v, buf, tid);
+                exchange<0, 1>(v, buf, tid, !CUT);
             }
             if (SC != SC_L0) {
                 rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                if (LAY == 0) exchange<1, 0>(v, buf, tid);
+                if (LAY == 0) exchange<1, 0>(v, buf, tid, true);
             }
         }
+        // The cut constants again for the outputs that need them (read back
+        // instead of held in registers through the rounds above).
+        if (EX != EX_NONE) cut_consts(cbase, g0, g1, g2, g3);
         if (EX == EX_DIAG) {
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
-                __stcs(A.diag + base + thr_off + offtab[r], (double)cr);
+                __stcs(A.diag + base + thr_off + off0(r), (double)cr);
             }
         }
         if (ACC) {
@@ -452,7 +562,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
                 if (EX == EX_COSTATE) {
                     const double c = (double)cr;
-                    __stcs(A.sv2 + base + thr_off + offtab[r], make_double2(c * v[r].x, c * v[r].y));
+                    __stcs(A.sv2 + base + thr_off + off0(r), make_double2(c * v[r].x, c * v[r].y));
                 }
             }
             const double y = ts - comp;
@@ -463,11 +573,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         if (ST) {
             if (LAY == 0) {
 #pragma unroll
-                for (int r = 0; r < kRegs; r++) __stcs(p + offtab[r], v[r]);
+                for (int r = 0; r < kRegs; r++) __stcs(p + off0(r), v[r]);
             } else {
                 double2* const p1 = A.sv + base + thr_off1;
 #pragma unroll
-                for (int r = 0; r < kRegs; r++) __stcs(p1 + offtab[kRegs + r], v[r]);
+                for (int r = 0; r < kRegs; r++) __stcs(p1 + off1(r), v[r]);
             }
         }
     }
