@@ -70,6 +70,7 @@ def parse_args(argv=None):
     ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the served-stream leg (0: skip it)")
     ap.add_argument("--serve-lanes", type=int, default=4)
+    ap.add_argument("--no-grad", action="store_true", help="skip the adjoint-gradient leg")
     return ap.parse_args(argv)
 
 
@@ -382,6 +383,9 @@ def run_ours(args):
     if not args.no_ref_schedule:
         line["reference_schedule"] = reference_schedule_leg(ctx, args, graphs[0], gammas, betas,
                                                             peak)
+    # ---- adjoint gradient of the N=26 p=10 circuit (one GPU)
+    if not args.no_grad and d.world == 1:
+        line["gradient"] = gradient_leg(ctx, peak)
     # ---- served energy+gradient stream vs sequential plain calls (one GPU)
     if args.serve_requests > 0 and d.world == 1:
         line["serving"] = serving_leg(args)
@@ -392,6 +396,37 @@ def run_ours(args):
     if d.rank == 0:
         print(json.dumps(line), flush=True)
     d.close()
+
+
+def gradient_leg(ctx, peak, n=26, P=10, reps=5):
+    """<C> and its 2p partial derivatives (adjoint method) for K_26 with
+    integer weights 1..10 and p=10: ms per evaluation and the adjoint
+    kernel's HBM GB/s (64 B per amplitude per launch: both vectors read and
+    written)."""
+    rng = np.random.default_rng(2610)
+    W = np.triu(rng.integers(1, 11, size=(n, n)).astype(np.float64), 1)
+    g, b = rng.uniform(0, np.pi, P), rng.uniform(0, np.pi / 2, P)
+    sv, cs = ctx.state(n), ctx.state(n)
+    try:
+        ctx.energy_grad(n, W, g, b, sv=sv, costate=cs)  # warm-up
+        ctx.profile_reset()
+        ctx.set_profiling(True)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            e, gg, gb = ctx.energy_grad(n, W, g, b, sv=sv, costate=cs)
+        wall = (time.perf_counter() - t0) / reps
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+    finally:
+        sv.free()
+        cs.free()
+    out = {"workload": f"K_{n} integer weights 1..10, p={P}, <C> + {2 * P} derivatives",
+           "ms_per_eval": 1000.0 * wall, "energy": e, "kernels": {}}
+    for kind, (kms, kn, kb) in prof.items():
+        gbs = kb / (kms / 1000.0) / 1e9 if kb else None
+        out["kernels"][kind] = {"launches": kn // reps, "ms_per_eval": kms / reps, "gbs": gbs,
+                                "frac": gbs / peak if gbs else None}
+    return out
 
 
 def serving_leg(args):

@@ -287,43 +287,37 @@ __device__ __forceinline__ void phase_bit(double2 (&v)[kRegs], int k, double2 E)
         if ((r >> k) & 1) v[r] = cmul(v[r], E);
 }
 
-template <typename WT, int PH, int GM, int EX, bool ST, int SC>
-__global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    using SM = PassSmem<WT>;
-    double2* buf = reinterpret_cast<double2*>(smraw);
-    unsigned char* const sm = smraw + sizeof(double2) * kTile;
-    double* red = reinterpret_cast<double*>(sm + SM::red);
-    WT* ke = reinterpret_cast<WT*>(sm + SM::ke);      // 2 x 32: [0] = K, [1+u] = e_u
-    WT* creg = reinterpret_cast<WT*>(sm + SM::creg);  // cut among the register bits
-    WT* Dm = reinterpret_cast<WT*>(sm + SM::Dm);
-    WT* Ru = reinterpret_cast<WT*>(sm + SM::Ru);
-    WT* wf = reinterpret_cast<WT*>(sm + SM::wf);      // wf[i][j] = w(fixed i, fixed j)
-    WT* wu = reinterpret_cast<WT*>(sm + SM::wu);      // wu[u][j] = w(tile u, fixed j)
-    WT* thrc = reinterpret_cast<WT*>(sm + SM::thrc);  // per-thread cut constants
-    double2* qtab = reinterpret_cast<double2*>(sm + SM::qtab);
-    double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
-    const int N = A.N, l = A.l, a = A.a;
-    const int nF = N - kTileBits;
-    constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
-    constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
-    constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
-    constexpr bool INTW = sizeof(WT) == sizeof(int);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
-    // Product-tree phases: FP64 weights always, integer weights with the
-    // two-level table (nhi == 0 keeps one global-table lookup per amplitude).
-    const bool tree = PH != PH_NONE && (!INTW || A.nhi > 0);
+// Shared-memory tables of the cut decomposition for one pass geometry.
+template <typename WT>
+struct CutTables {
+    WT* ke;        // 2 x 32, double-buffered per tile: [0] = K, [1+u] = e_u
+    WT* creg;      // 16: cut among the 4 register bits (layout L0)
+    WT* Dm;        // nF: sum of weights between fixed bit m and the tile bits
+    WT* Ru;        // 12: sum of weights between tile bit u and the fixed bits
+    WT* wf;        // wf[i * kWfStride + j] = w(fixed i, fixed j)
+    WT* wu;        // wu[u * kWfStride + j] = w(tile u, fixed j)
+    WT* thrc;      // 5 x 256 per-thread constants: [0] cut among the thread's
+                   // 8 tile bits (plus their edges to set register bits),
+                   // [1+k] = f_k, the thread's part of g_k
+    double2* qtab; // 16: z^creg[r], z = exp(i*gamma) (phase passes)
 
-    // ---- set-up: compact weight tables of this pass's tile geometry
-    WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
-    if (CUT) {
-        const WT* gw = reinterpret_cast<const WT*>(A.w);
-        for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
+    __device__ CutTables(unsigned char* sm) {
+        using SM = PassSmem<WT>;
+        ke = reinterpret_cast<WT*>(sm + SM::ke);
+        creg = reinterpret_cast<WT*>(sm + SM::creg);
+        Dm = reinterpret_cast<WT*>(sm + SM::Dm);
+        Ru = reinterpret_cast<WT*>(sm + SM::Ru);
+        wf = reinterpret_cast<WT*>(sm + SM::wf);
+        wu = reinterpret_cast<WT*>(sm + SM::wu);
+        thrc = reinterpret_cast<WT*>(sm + SM::thrc);
+        qtab = reinterpret_cast<double2*>(sm + SM::qtab);
     }
-    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, tid, kPassThreads);
-    __syncthreads();
-    if (CUT) {
+
+    // Fill the tables from the N*N weights sw (shared memory, all threads;
+    // the caller synchronises before and after).  QT: also z^creg[r].
+    template <bool QT>
+    __device__ void setup(const WT* sw, int N, int l, int a, int tid, double gamma) const {
+        const int nF = N - kTileBits;
         for (int idx = tid; idx < nF * nF; idx += kPassThreads) {
             const int i = idx / nF, j = idx - i * nF;
             wf[i * kWfStride + j] = sw[fixed_phys(i, l, a) * N + fixed_phys(j, l, a)];
@@ -350,15 +344,12 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                     if (((r >> k) ^ (r >> k2)) & 1)
                         c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
             creg[r] = c;
-            if (PH != PH_NONE) {
+            if (QT) {
                 double sn, cs;
-                sincos(A.gamma * (double)c, &sn, &cs);
+                sincos(gamma * (double)c, &sn, &cs);
                 qtab[r] = make_double2(cs, sn);
             }
         }
-        // Per-thread constants of the cut decomposition (layout L0), kept in
-        // shared memory: thrc[0] = cut among the thread's 8 tile bits plus
-        // their edges to set register bits, thrc[1+k] = f_k.
         WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
         for (int j = 0; j < 8; j++) {
             const int pj = tile_phys(j, l, a);
@@ -387,6 +378,100 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         thrc[3 * kPassThreads + tid] = f2;
         thrc[4 * kPassThreads + tid] = f3;
     }
+
+    // K and e_u of the tile at `base` into kp (warps 0 and 1 of the block;
+    // the caller synchronises before reading kp).
+    __device__ void tile(WT* kp, i64 base, int nF, int l, int a, int warp, int lane) const {
+        if (warp >= 2) return;
+        const int zi = lane < nF ? (int)((base >> fixed_phys(lane, l, a)) & 1) : 0;
+        const unsigned F = __ballot_sync(0xffffffffu, zi);
+        if (warp == 0) {
+            WT h = 0;
+            if (lane < nF) {
+                if (zi) h = Dm[lane];
+                const WT* row = wf + lane * kWfStride;
+#pragma unroll
+                for (int j = 1; j < kMaxFixed; j++)
+                    if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi)) h += row[j];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+            if (lane == 0) kp[0] = h;
+        } else if (lane < kTileBits) {
+            WT e = Ru[lane];
+            const WT* row = wu + lane * kWfStride;
+#pragma unroll
+            for (int j = 0; j < kMaxFixed; j++)
+                if (j < nF && ((F >> j) & 1u)) e -= 2 * row[j];
+            kp[1 + lane] = e;
+        }
+    }
+
+    // cb = cut value of the thread's register slot 0, g_k = change of the
+    // cut when register bit k is set; slot r has c_r = cb + creg[r] +
+    // sum_k r_k g_k.
+    __device__ void consts(const WT* kp, int tid, WT& cb, WT& g0, WT& g1, WT& g2, WT& g3) const {
+        cb = kp[0] + thrc[tid];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            if ((tid >> j) & 1) cb += kp[1 + j];
+        g0 = thrc[kPassThreads + tid] + kp[9];
+        g1 = thrc[2 * kPassThreads + tid] + kp[10];
+        g2 = thrc[3 * kPassThreads + tid] + kp[11];
+        g3 = thrc[4 * kPassThreads + tid] + kp[12];
+    }
+};
+
+// z^d with z = exp(i*gamma): the two-level table (integer weights) or sincos.
+template <typename WT>
+__device__ __forceinline__ double2 zpow(const PassArgs& A, const double2* smtab, WT d) {
+    if (sizeof(WT) == sizeof(int)) return tab_pow(A, smtab, (int)d);
+    double sn, cs;
+    sincos(A.gamma * (double)d, &sn, &cs);
+    return make_double2(cs, sn);
+}
+
+// P = phase(cbase) without the layer-0 scale: ph0 * z^cbase (integer
+// weights) or scale * exp(i*gamma*(cbase - W/2)).
+template <typename WT>
+__device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* smtab, WT cbase) {
+    if (sizeof(WT) == sizeof(int))
+        return cmul(make_double2(A.ph0x, A.ph0y), tab_pow(A, smtab, (int)cbase));
+    double sn, cs;
+    sincos(A.gamma * ((double)cbase - 0.5 * A.W), &sn, &cs);
+    return make_double2(cs * A.scale, sn * A.scale);
+}
+
+template <typename WT, int PH, int GM, int EX, bool ST, int SC>
+__global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using SM = PassSmem<WT>;
+    double2* buf = reinterpret_cast<double2*>(smraw);
+    unsigned char* const sm = smraw + sizeof(double2) * kTile;
+    double* red = reinterpret_cast<double*>(sm + SM::red);
+    const CutTables<WT> ct(sm);
+    double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
+    const int N = A.N, l = A.l, a = A.a;
+    const int nF = N - kTileBits;
+    constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
+    constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
+    constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
+    constexpr bool INTW = sizeof(WT) == sizeof(int);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
+    // Product-tree phases: FP64 weights always, integer weights with the
+    // two-level table (nhi == 0 keeps one global-table lookup per amplitude).
+    const bool tree = PH != PH_NONE && (!INTW || A.nhi > 0);
+
+    // ---- set-up: compact weight tables of this pass's tile geometry
+    WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
+    if (CUT) {
+        const WT* gw = reinterpret_cast<const WT*>(A.w);
+        for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
+    }
+    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, tid, kPassThreads);
+    __syncthreads();
+    if (CUT) ct.template setup<PH != PH_NONE>(sw, N, l, a, tid, A.gamma);
     __syncthreads();  // the weights in buf are dead from here on
 
     // Address pieces: the thread's offsets in layouts L0 and L1 and the
@@ -443,77 +528,26 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                 }
             }
         }
-        // cbase = cut value of the thread's slot 0, g_k = change when register
-        // bit k is set (from this tile's K, e_u and the thread's constants).
-        WT* const kp = ke + 32 * par;
-        auto cut_consts = [&](WT& cb, WT& h0, WT& h1, WT& h2, WT& h3) {
-            cb = kp[0] + thrc[tid];
-#pragma unroll
-            for (int j = 0; j < 8; j++)
-                if ((tid >> j) & 1) cb += kp[1 + j];
-            h0 = thrc[kPassThreads + tid] + kp[9];
-            h1 = thrc[2 * kPassThreads + tid] + kp[10];
-            h2 = thrc[3 * kPassThreads + tid] + kp[11];
-            h3 = thrc[4 * kPassThreads + tid] + kp[12];
-        };
+        WT* const kp = ct.ke + 32 * par;  // double-buffered: no barrier for the previous readers
         WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
         if (CUT) {
-            // K and e_u of this tile (warps 0 and 1), double-buffered so the
-            // previous tile's readers need no barrier of their own.
-            if (warp < 2) {
-                const int zi = lane < nF ? (int)((base >> fixed_phys(lane, l, a)) & 1) : 0;
-                const unsigned F = __ballot_sync(0xffffffffu, zi);
-                if (warp == 0) {
-                    WT h = 0;
-                    if (lane < nF) {
-                        if (zi) h = Dm[lane];
-                        const WT* row = wf + lane * kWfStride;
-#pragma unroll
-                        for (int j = 1; j < kMaxFixed; j++)
-                            if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi))
-                                h += row[j];
-                    }
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-                    if (lane == 0) kp[0] = h;
-                } else if (lane < kTileBits) {
-                    WT e = Ru[lane];
-                    const WT* row = wu + lane * kWfStride;
-#pragma unroll
-                    for (int j = 0; j < kMaxFixed; j++)
-                        if (j < nF && ((F >> j) & 1u)) e -= 2 * row[j];
-                    kp[1 + lane] = e;
-                }
-            }
+            ct.tile(kp, base, nF, l, a, warp, lane);
             __syncthreads();
-            cut_consts(cbase, g0, g1, g2, g3);
+            ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }
         if (PH != PH_NONE) {
             if (tree) {
-                auto zpow = [&](WT d) -> double2 {  // z^d
-                    if (INTW) return tab_pow(A, smtab, (int)d);
-                    double sn, cs;
-                    sincos(A.gamma * (double)d, &sn, &cs);
-                    return make_double2(cs, sn);
-                };
-                double2 P;
-                if (INTW) {
-                    P = cmul(make_double2(A.ph0x, A.ph0y), tab_pow(A, smtab, (int)cbase));
-                    if (PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
-                } else {
-                    double sn, cs;
-                    sincos(A.gamma * ((double)cbase - 0.5 * A.W), &sn, &cs);
-                    P = make_double2(cs * A.scale, sn * A.scale);
-                }
-                phase_base<PH>(v, P, qtab);
-                phase_bit(v, 0, zpow(g0));
-                phase_bit(v, 1, zpow(g1));
-                phase_bit(v, 2, zpow(g2));
-                phase_bit(v, 3, zpow(g3));
+                double2 P = phase_of<WT>(A, smtab, cbase);
+                if (INTW && PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
+                phase_base<PH>(v, P, ct.qtab);
+                phase_bit(v, 0, zpow<WT>(A, smtab, g0));
+                phase_bit(v, 1, zpow<WT>(A, smtab, g1));
+                phase_bit(v, 2, zpow<WT>(A, smtab, g2));
+                phase_bit(v, 3, zpow<WT>(A, smtab, g3));
             } else {
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) +
+                    const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
                                   ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
                                   ((r & 8) ? g3 : WT(0));
                     const double2 ph = int_phase(A, smtab, (int)cr);
@@ -544,11 +578,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         }
         // The cut constants again for the outputs that need them (read back
         // instead of held in registers through the rounds above).
-        if (EX != EX_NONE) cut_consts(cbase, g0, g1, g2, g3);
+        if (EX != EX_NONE) ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         if (EX == EX_DIAG) {
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 __stcs(A.diag + base + thr_off + off0(r), (double)cr);
             }
@@ -557,7 +591,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             double ts = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
                 if (EX == EX_COSTATE) {

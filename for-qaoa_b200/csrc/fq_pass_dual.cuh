@@ -67,8 +67,8 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
 
 template <int LF, int LT>
 __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[kRegs],
-                                              double2* buf, int tid) {
-    __syncthreads();
+                                              double2* buf, int tid, bool wait_readers = true) {
+    if (wait_readers) __syncthreads();  // previous readers of buf are done
 #pragma unroll
     for (int r = 0; r < kRegs; r++) {
         const int sl = xslot(lay_index<LF>(tid, r));
@@ -84,198 +84,172 @@ __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[
     }
 }
 
+// Shared memory: two 64 KB exchange buffers (the weights are staged in them
+// while the kernel sets up), then the tables of k_pass.
 template <typename WT>
-__host__ __device__ inline size_t dual_smem_bytes(int N) {
-    return 2 * sizeof(double2) * kTile + sizeof(double) * 16 + sizeof(i64) * 32 +
-           sizeof(int) * 24 + sizeof(WT) * (N * N + 32 + 16 + 24 + 16) + 16 + phase_smem_bytes();
+__host__ __device__ inline size_t dual_smem_bytes(int) {
+    return 2 * sizeof(double2) * kTile + PassSmem<WT>::bytes + 16 * sizeof(double);
+}
+
+// v *= conj(P * Q_r) on every slot, then conj(E) on the slots with bit k:
+// the inverse of the phase applied by k_pass (see phase_base / phase_bit).
+__device__ __forceinline__ void unphase_base(double2 (&v)[kRegs], double2 (&w)[kRegs], double2 P,
+                                             const double2* qtab) {
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) {
+        const double2 ph = cmul(P, qtab[r]);
+        const double2 c = make_double2(ph.x, -ph.y);
+        v[r] = cmul(v[r], c);
+        w[r] = cmul(w[r], c);
+    }
+}
+
+__device__ __forceinline__ void unphase_bit(double2 (&v)[kRegs], double2 (&w)[kRegs], int k,
+                                            double2 E) {
+    const double2 c = make_double2(E.x, -E.y);
+#pragma unroll
+    for (int r = 0; r < kRegs; r++)
+        if ((r >> k) & 1) {
+            v[r] = cmul(v[r], c);
+            w[r] = cmul(w[r], c);
+        }
 }
 
 // PHI: this pass also accumulates dE/dgamma (-Im<w|S|v>, negated on the
 // host) and, if A.scale != 0, multiplies both vectors by the conjugate
 // phase.  ST: write the vectors back.  Partials: gb[blockIdx] (beta) and
-// gg[blockIdx] (gamma).
+// gg[blockIdx] (gamma).  The next tile of both vectors is prefetched into
+// L2 while the current one is computed (one CTA per SM cannot hide the
+// HBM latency of its loads otherwise).
 template <typename WT, bool PHI, int SC, bool ST>
 __global__ void __launch_bounds__(kPassThreads, 1)
     k_pass_dual(const PassArgs A, double* gb, double* gg) {
     extern __shared__ __align__(16) unsigned char smraw[];
+    using SM = PassSmem<WT>;
     double2* buf = reinterpret_cast<double2*>(smraw);
-    double* red = reinterpret_cast<double*>(buf + 2 * kTile);  // 16
-    i64* offtab = reinterpret_cast<i64*>(red + 16);
-    int* fpos = reinterpret_cast<int*>(offtab + 32);
-    WT* sw = reinterpret_cast<WT*>(fpos + 24);
-    WT* ke = sw + A.N * A.N;
-    WT* creg = ke + 32;
-    WT* Dm = creg + 16;
-    WT* Ru = Dm + 24;
-    double2* smtab = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);
+    unsigned char* const sm = smraw + 2 * sizeof(double2) * kTile;
+    const CutTables<WT> ct(sm);
+    double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
+    double* red = reinterpret_cast<double*>(sm + SM::bytes);  // 16: beta and gamma partials
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
     const int nmid = a - l;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr bool CUT = PHI;
+    constexpr bool INTW = sizeof(WT) == sizeof(int);
 
-    if (tid < 2 * kRegs) {
-        const int r = tid & 15, lo = tid < kRegs ? 8 : 4;
-        i64 o = 0;
-        for (int k = 0; k < 4; k++)
-            if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
-        offtab[tid] = o;
-    }
+    WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
     if (CUT) {
         const WT* gw = reinterpret_cast<const WT*>(A.w);
         for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
-        if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
-        if (sizeof(WT) == sizeof(int)) load_phase_tables(A, smtab, tid, kPassThreads);
+        if (INTW) load_phase_tables(A, smtab, tid, kPassThreads);
     }
     __syncthreads();
-    if (CUT) {
-        if (tid < nF) {
-            const int m = fpos[tid];
-            WT d = 0;
-            for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
-            Dm[tid] = d;
-        } else if (tid >= 32 && tid < 32 + kTileBits) {
-            const int u = tile_phys(tid - 32, l, a);
-            WT r = 0;
-            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
-            Ru[tid - 32] = r;
-        } else if (tid >= 64 && tid < 80) {
-            const int r = tid - 64;
-            WT c = 0;
-            for (int k = 0; k < 4; k++)
-                for (int k2 = k + 1; k2 < 4; k2++)
-                    if (((r >> k) ^ (r >> k2)) & 1)
-                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
-            creg[r] = c;
-        }
-    }
-    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
-    if (CUT) {
-        for (int j = 0; j < 8; j++) {
-            const int pj = tile_phys(j, l, a);
-            const int tj = (tid >> j) & 1;
-            for (int j2 = j + 1; j2 < 8; j2++)
-                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
-            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
-            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
-            if (tj) {
-                athr += w0 + w1 + w2 + w3;
-                f0 -= w0;
-                f1 -= w1;
-                f2 -= w2;
-                f3 -= w3;
-            } else {
-                f0 += w0;
-                f1 += w1;
-                f2 += w2;
-                f3 += w3;
-            }
-        }
-    }
-    i64 thr_off = 0, thr_off1 = 0;
-    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    {
-        const int t1 = lay_index<1>(tid, 0);
-        for (int j = 0; j < kTileBits; j++)
-            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
-    }
+    if (CUT) ct.template setup<true>(sw, N, l, a, tid, A.gamma);
+    __syncthreads();  // the weights in buf are dead from here on
+
+    const i64 thr_off = tile_off(tid, l, a);
+    const i64 thr_off1 = tile_off(lay_index<1>(tid, 0), l, a);
+    const i64 s8 = 1ll << tile_phys(8, l, a), s9 = 1ll << tile_phys(9, l, a);
+    const i64 s10 = 1ll << tile_phys(10, l, a), s11 = 1ll << tile_phys(11, l, a);
+    const i64 s4 = 1ll << tile_phys(4, l, a), s5 = 1ll << tile_phys(5, l, a);
+    const i64 s6 = 1ll << tile_phys(6, l, a), s7 = 1ll << tile_phys(7, l, a);
+    auto off0 = [&](int r) -> i64 {
+        return ((r & 1) ? s8 : 0) + ((r & 2) ? s9 : 0) + ((r & 4) ? s10 : 0) + ((r & 8) ? s11 : 0);
+    };
+    auto off1 = [&](int r) -> i64 {
+        return ((r & 1) ? s4 : 0) + ((r & 2) ? s5 : 0) + ((r & 4) ? s6 : 0) + ((r & 8) ? s7 : 0);
+    };
+    auto tile_base = [&](i64 T) -> i64 {
+        return ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+    };
+    const bool contiguous = (l == kTileBits);
+    const int pf_step = l < 3 ? l : 3;
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double accb = 0, accg = 0;
 
-    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x) {
-        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
-        if (CUT) {
-            __syncthreads();
-            if (warp == 0) {
-                WT h = 0;
-                if (lane < nF) {
-                    const int m = fpos[lane];
-                    const int zm = (int)((base >> m) & 1);
-                    if (zm) h += Dm[lane];
-                    for (int i = lane + 1; i < nF; i++)
-                        if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-                if (lane < kTileBits) {
-                    const int u = tile_phys(lane, l, a);
-                    WT e = Ru[lane];
-                    for (int i = 0; i < nF; i++)
-                        if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
-                    ke[1 + lane] = e;
-                }
-                if (lane == 0) ke[0] = h;
-            }
-            __syncthreads();
-        }
+    int par = 0;
+    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
+        const i64 base = tile_base(T);
         double2* const pv = A.sv + base + thr_off;
         double2* const pw = A.sv2 + base + thr_off;
         double2 v[kRegs], w[kRegs];
 #pragma unroll
         for (int r = 0; r < kRegs; r++) {
-            v[r] = __ldcs(pv + offtab[r]);
-            w[r] = __ldcs(pw + offtab[r]);
+            v[r] = __ldcs(pv + off0(r));
+            w[r] = __ldcs(pw + off0(r));
         }
+        if (T + gridDim.x < A.ntiles) {
+            const i64 b2 = tile_base(T + gridDim.x);
+            if (contiguous) {
+                if (tid < 2)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
+                                     (tid ? A.sv2 : A.sv) + b2),
+                                 "r"((unsigned)(kTile * sizeof(double2)))
+                                 : "memory");
+            } else {
+                for (int j = tid; j < (1 << (kTileBits - pf_step)); j += kPassThreads) {
+                    const i64 o = b2 + tile_off(j << pf_step, l, a);
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + o) : "memory");
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv2 + o) : "memory");
+                }
+            }
+        }
+        WT* const kp = ct.ke + 32 * par;
+        if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // read after the exchanges' barriers
         rx_regs_dual(v, w, m_hi, A.c, A.s, accb);
         if (lo_lane >= 0) rx_lane_dual(v, w, lo_lane, A.c, A.s, accb);
+        // The previous tile's readers of buf are done once every thread is
+        // past this tile's first barrier: with the cut barrier (CUT) or the
+        // leading barrier of the first exchange.
         if (SC == SC_L021) {
-            exchange_dual<0, 2>(v, w, buf, tid);
+            exchange_dual<0, 2>(v, w, buf, tid, true);
             rx_regs_dual(v, w, m_lo, A.c, A.s, accb);
-            exchange_dual<2, 1>(v, w, buf, tid);
+            exchange_dual<2, 1>(v, w, buf, tid, true);
         } else if (SC == SC_L01) {
-            exchange_dual<0, 1>(v, w, buf, tid);
+            exchange_dual<0, 1>(v, w, buf, tid, true);
         }
         constexpr int LAY = (SC != SC_L0 && !PHI) ? 1 : 0;
         if (SC != SC_L0) {
             rx_regs_dual(v, w, m_mid, A.c, A.s, accb);
-            if (LAY == 0) exchange_dual<1, 0>(v, w, buf, tid);
+            if (LAY == 0) exchange_dual<1, 0>(v, w, buf, tid, true);
         }
         if (PHI) {
-            WT cbase = ke[0] + athr;
-#pragma unroll
-            for (int jj = 0; jj < 8; jj++)
-                if ((tid >> jj) & 1) cbase += ke[1 + jj];
-            const WT g0 = f0 + ke[9], g1 = f1 + ke[10], g2 = f2 + ke[11], g3 = f3 + ke[12];
+            if (SC == SC_L0) __syncthreads();  // kp written by warps 0 and 1
+            WT cbase, g0, g1, g2, g3;
+            ct.consts(kp, tid, cbase, g0, g1, g2, g3);
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
-                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
+                              ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
+                              ((r & 8) ? g3 : WT(0));
                 const double S = 2.0 * (double)cr - A.W;
                 accg = fma(w[r].x * v[r].y - w[r].y * v[r].x, S, accg);
-                if (A.scale != 0.0) {
-                    double2 ph;
-                    if (sizeof(WT) == sizeof(int)) {
-                        ph = int_phase(A, smtab, (int)cr);
-                    } else {
-                        double sn, cs;
-                        sincos(S * A.gamma / 2, &sn, &cs);
-                        ph = make_double2(cs, sn);
-                    }
-                    // multiply by conj(ph)
-                    const double2 a0 = v[r], b0 = w[r];
-                    v[r].x = a0.x * ph.x + a0.y * ph.y;
-                    v[r].y = a0.y * ph.x - a0.x * ph.y;
-                    w[r].x = b0.x * ph.x + b0.y * ph.y;
-                    w[r].y = b0.y * ph.x - b0.x * ph.y;
-                }
+            }
+            if (A.scale != 0.0) {
+                const double2 P = phase_of<WT>(A, smtab, cbase);
+                unphase_base(v, w, P, ct.qtab);
+                unphase_bit(v, w, 0, zpow<WT>(A, smtab, g0));
+                unphase_bit(v, w, 1, zpow<WT>(A, smtab, g1));
+                unphase_bit(v, w, 2, zpow<WT>(A, smtab, g2));
+                unphase_bit(v, w, 3, zpow<WT>(A, smtab, g3));
             }
         }
         if (ST) {
             if (LAY == 0) {
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    __stcs(pv + offtab[r], v[r]);
-                    __stcs(pw + offtab[r], w[r]);
+                    __stcs(pv + off0(r), v[r]);
+                    __stcs(pw + off0(r), w[r]);
                 }
             } else {
                 double2* const qv = A.sv + base + thr_off1;
                 double2* const qw = A.sv2 + base + thr_off1;
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    __stcs(qv + offtab[kRegs + r], v[r]);
-                    __stcs(qw + offtab[kRegs + r], w[r]);
+                    __stcs(qv + off1(r), v[r]);
+                    __stcs(qw + off1(r), w[r]);
                 }
             }
         }

@@ -51,6 +51,61 @@ def angles(rng, P):
     return rng.uniform(0, np.pi, P), rng.uniform(0, np.pi / 2, P)
 
 
+# ---- light cones: <C> of a large state from small exact simulations ------
+def random_regular(n, d, rng):
+    """Seeded pairing model, retried until the graph is simple."""
+    while True:
+        stubs = rng.permutation(np.repeat(np.arange(n), d))
+        pairs = stubs.reshape(-1, 2)
+        if np.any(pairs[:, 0] == pairs[:, 1]):
+            continue
+        e = {tuple(sorted(p)) for p in pairs.tolist()}
+        if len(e) == len(pairs):
+            return sorted(e)
+
+
+def weighted_graph(n, edges, rng):
+    W = np.zeros((n, n))
+    for u, v in edges:
+        W[u, v] = rng.random()
+    return W
+
+
+def ball(adj, seeds, r):
+    cur = set(seeds)
+    for _ in range(r):
+        cur |= {x for u in cur for x in adj[u]}
+    return cur
+
+
+def light_cone_energy(oracle, n, edges, W, gammas, betas):
+    """<C> after p QAOA layers as a sum of edge terms, each simulated by the
+    oracle on the edges within distance p-1 of the edge (its light cone)."""
+    p = len(gammas)
+    adj = {u: set() for u in range(n)}
+    for u, v in edges:
+        adj[u].add(v)
+        adj[v].add(u)
+    total = 0.0
+    for u, v in edges:
+        inner = ball(adj, (u, v), p - 1)
+        sub_edges = [(a, b) for a, b in edges if a in inner or b in inner]
+        nodes = sorted({x for e in sub_edges for x in e})
+        idx = {x: i for i, x in enumerate(nodes)}
+        m = len(nodes)
+        Ws = np.zeros((m, m))
+        for a, b in sub_edges:
+            i, j = sorted((idx[a], idx[b]))
+            Ws[i, j] = W[a, b]
+        psi = oracle.qaoa_logical(Ws, gammas, betas)
+        z = np.arange(1 << m)
+        par = ((z >> idx[u]) ^ (z >> idx[v])) & 1
+        zz = np.sum(np.abs(psi) ** 2 * (1 - 2 * par))
+        total += W[u, v] * (1 - zz) / 2
+    return total
+
+
+
 @pytest.fixture(scope="session")
 def oracle():
     import oracle as O

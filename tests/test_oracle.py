@@ -138,3 +138,16 @@ def test_swap_and_relabel_are_involutions(oracle):
     W = complete_int(N, rng)
     g2 = oracle.mapping_after_swap_conti(oracle.mapping_after_swap_conti(W, 0, 4, 3), 0, 4, 3)
     assert np.array_equal(g2, W)
+
+
+@pytest.mark.parametrize("n,p", [(12, 1), (12, 2), (10, 3)])
+def test_light_cone_energy_matches_full_state(oracle, n, p):
+    """The light-cone sum that checks the 32-qubit GPU run equals the full
+    oracle simulation where both fit."""
+    from conftest import light_cone_energy, random_regular, weighted_graph
+    rng = np.random.default_rng(100 + n + p)
+    edges = random_regular(n, 3, rng)
+    W = weighted_graph(n, edges, rng)
+    g, b = rng.uniform(0, np.pi, p), rng.uniform(0, np.pi / 2, p)
+    full = oracle.expectation(oracle.qaoa_logical(W, g, b), W)
+    assert abs(light_cone_energy(oracle, n, edges, W, g, b) - full) <= 1e-13 * abs(full)
