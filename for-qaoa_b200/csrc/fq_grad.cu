@@ -15,9 +15,9 @@
 
 namespace fq {
 
-template <typename WT, bool PHI, int SC>
+template <typename WT, bool PHI, int SC, int GM>
 static int launch_dual(fq_ctx* ctx, const PassArgs& A, double* gb, double* gg) {
-    auto fn = k_pass_dual<WT, PHI, SC, true>;
+    auto fn = k_pass_dual<WT, PHI, SC, true, GM>;
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)dual_smem_bytes<WT>(kMaxQubits)));
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
@@ -29,18 +29,25 @@ static int launch_dual(fq_ctx* ctx, const PassArgs& A, double* gb, double* gg) {
     return FQ_OK;
 }
 
-static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, const PassArgs& A, double* gb,
-                         double* gg) {
+template <int GM>
+static int dispatch_dual_gm(fq_ctx* ctx, bool integer, bool phi, const PassArgs& A, double* gb,
+                            double* gg) {
     if (phi) {
         FQ_CHECK(schedule_for(A.tmask) == SC_L021, FQ_ERR_INVALID, "adjoint phase pass mask");
-        return integer ? launch_dual<int, true, SC_L021>(ctx, A, gb, gg)
-                       : launch_dual<double, true, SC_L021>(ctx, A, gb, gg);
+        return integer ? launch_dual<int, true, SC_L021, GM>(ctx, A, gb, gg)
+                       : launch_dual<double, true, SC_L021, GM>(ctx, A, gb, gg);
     }
     switch (schedule_for(A.tmask)) {
-        case SC_L021: return launch_dual<int, false, SC_L021>(ctx, A, gb, gg);
-        case SC_L01: return launch_dual<int, false, SC_L01>(ctx, A, gb, gg);
-        default: return launch_dual<int, false, SC_L0>(ctx, A, gb, gg);
+        case SC_L021: return launch_dual<int, false, SC_L021, GM>(ctx, A, gb, gg);
+        case SC_L01: return launch_dual<int, false, SC_L01, GM>(ctx, A, gb, gg);
+        default: return launch_dual<int, false, SC_L0, GM>(ctx, A, gb, gg);
     }
+}
+
+static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, int gm, const PassArgs& A,
+                         double* gb, double* gg) {
+    return gm == GM_TAN ? dispatch_dual_gm<GM_TAN>(ctx, integer, phi, A, gb, gg)
+                        : dispatch_dual_gm<GM_COT>(ctx, integer, phi, A, gb, gg);
 }
 
 int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream) {
@@ -154,9 +161,15 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
                                ctx->d_result));
     }
     // Reverse sweep: per layer the strided passes, then the contiguous pass
-    // with dE/dgamma and the inverse phase.
+    // with dE/dgamma and the inverse phase.  RX(-beta) runs in reduced form
+    // f * G (gate_params): the kernels track the scale the vectors gain
+    // (1/f per rotation) and the contiguous pass multiplies f^N back in.
     double* gb = ctx->d_partial;
     for (int k = P - 1; k >= 0; k--) {
+        int gm;
+        double gx, f;
+        gate_params(-betas[k], gm, gx, f);
+        int rotated = 0;  // qubits rotated so far in this layer's reverse sweep
         const int nhi = g.integer ? engine_nhi(g) : 0;
         if (g.integer) {
             if (nhi > 0)
@@ -171,14 +184,17 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             A.l = plan[i].l;
             A.a = plan[i].a;
             A.tmask = plan[i].tmask;
-            A.c = cos(betas[k] / 2);
-            A.s = -sin(betas[k] / 2);  // RX(-beta)
+            A.gx = gx;
+            A.f2 = f * f;
+            A.sc0 = pow(f * f, rotated);
+            rotated += __builtin_popcount(plan[i].tmask);
             A.gamma = gammas[k];
             if (nhi > 0) set_table_args(A, g, gammas[k], 1.0);
-            A.scale = k > 0 ? 1.0 : 0.0;  // inverse phase only where layers remain
+            // Inverse phase (times f^N) only where layers remain.
+            A.scale = k > 0 ? pow(f, N) : 0.0;
             const int grid = (int)std::min<i64>(A.ntiles, ctx->num_sms);
             double* gg = gb + grid;
-            FQ_TRY(dispatch_dual(ctx, g.integer, i == 0, A, gb, gg));
+            FQ_TRY(dispatch_dual(ctx, g.integer, i == 0, gm, A, gb, gg));
             FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + 1 + P + k * npass + i));
             if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
         }

@@ -90,6 +90,8 @@ struct PassArgs {
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
     double W;        // total weight
     double scale;    // multiplies the phase
+    double sc0, f2;  // adjoint passes: scale of the inner products at the pass's start, and
+                     // the factor (f^2) it gains with every reduced rotation
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
     int* err;        // device error flag (bounded waits that gave up)
 };

@@ -25,30 +25,40 @@
 
 namespace fq {
 
-// RX on the register bits of m4 for both vectors; adds Im<w|X_q|v> of each
-// rotated qubit q to acc (taken before the rotation; it commutes).
+// Reduced RX (GM_TAN / GM_COT: the gate divided by its factor f) on the
+// register bits of m4 for both vectors.  Before each qubit q is rotated,
+// Im<w|X_q|v> is added to acc times sc, the scale that undoes the factors
+// 1/f the vectors picked up from the reduced rotations so far (X_q commutes
+// with every RX, so the true inner product is the same at any point of the
+// mixer); sc gains f^2 with every rotation.
+template <int GM>
 __device__ __forceinline__ void rx_regs_dual(double2 (&v)[kRegs], double2 (&w)[kRegs], unsigned m4,
-                                             double c, double s, double& acc) {
+                                             double g, double f2, double& sc, double& acc) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if ((m4 >> k) & 1u) {
+            double t = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 if (!((r >> k) & 1)) {
                     const int q = r | (1 << k);
-                    acc += (w[r].x * v[q].y - w[r].y * v[q].x) + (w[q].x * v[r].y - w[q].y * v[r].x);
-                    rx_pair<GM_FULL>(v[r], v[q], 0.0, c, s);
-                    rx_pair<GM_FULL>(w[r], w[q], 0.0, c, s);
+                    t += (w[r].x * v[q].y - w[r].y * v[q].x) + (w[q].x * v[r].y - w[q].y * v[r].x);
+                    rx_pair<GM>(v[r], v[q], g, 0.0, 0.0);
+                    rx_pair<GM>(w[r], w[q], g, 0.0, 0.0);
                 }
             }
+            acc = fma(sc, t, acc);
+            sc *= f2;
         }
     }
 }
 
 // The same for a qubit held in lane bit j (each lane adds its own term).
+template <int GM>
 __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[kRegs], int j,
-                                             double c, double s, double& acc) {
+                                             double g, double f2, double& sc, double& acc) {
     const unsigned lm = 1u << j;
+    double t = 0;
 #pragma unroll
     for (int r = 0; r < kRegs; r++) {
         double2 pv, pw;
@@ -56,13 +66,22 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
         pv.y = __shfl_xor_sync(0xffffffffu, v[r].y, lm);
         pw.x = __shfl_xor_sync(0xffffffffu, w[r].x, lm);
         pw.y = __shfl_xor_sync(0xffffffffu, w[r].y, lm);
-        acc += w[r].x * pv.y - w[r].y * pv.x;
+        t += w[r].x * pv.y - w[r].y * pv.x;
         const double2 mv = v[r], mw = w[r];
-        v[r].x = mv.x * c + pv.y * s;
-        v[r].y = mv.y * c - pv.x * s;
-        w[r].x = mw.x * c + pw.y * s;
-        w[r].y = mw.y * c - pw.x * s;
+        if (GM == GM_TAN) {
+            v[r].x = fma(g, pv.y, mv.x);
+            v[r].y = fma(-g, pv.x, mv.y);
+            w[r].x = fma(g, pw.y, mw.x);
+            w[r].y = fma(-g, pw.x, mw.y);
+        } else {
+            v[r].x = fma(g, mv.x, pv.y);
+            v[r].y = fma(g, mv.y, -pv.x);
+            w[r].x = fma(g, mw.x, pw.y);
+            w[r].y = fma(g, mw.y, -pw.x);
+        }
     }
+    acc = fma(sc, t, acc);
+    sc *= f2;
 }
 
 template <int LF, int LT>
@@ -115,13 +134,16 @@ __device__ __forceinline__ void unphase_bit(double2 (&v)[kRegs], double2 (&w)[kR
         }
 }
 
-// PHI: this pass also accumulates dE/dgamma (-Im<w|S|v>, negated on the
-// host) and, if A.scale != 0, multiplies both vectors by the conjugate
-// phase.  ST: write the vectors back.  Partials: gb[blockIdx] (beta) and
+// RX(-beta) in reduced form GM (A.gx = t or u, A.f2 = f^2, A.sc0 = scale of
+// the vectors at the pass's start, see rx_regs_dual).  PHI: this pass also
+// accumulates dE/dgamma (-Im<w|S|v>, negated on the host) and, if
+// A.scale != 0, multiplies both vectors by the conjugate phase times A.scale
+// = f^N, which returns them to their true scale for the next layer.  ST:
+// write the vectors back.  Partials: gb[blockIdx] (beta) and
 // gg[blockIdx] (gamma).  The next tile of both vectors is prefetched into
 // L2 while the current one is computed (one CTA per SM cannot hide the
 // HBM latency of its loads otherwise).
-template <typename WT, bool PHI, int SC, bool ST>
+template <typename WT, bool PHI, int SC, bool ST, int GM>
 __global__ void __launch_bounds__(kPassThreads, 1)
     k_pass_dual(const PassArgs A, double* gb, double* gg) {
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -168,6 +190,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double accb = 0, accg = 0;
+    const double g = A.gx, f2 = A.f2;
 
     int par = 0;
     for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
@@ -198,37 +221,41 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         }
         WT* const kp = ct.ke + 32 * par;
         if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // read after the exchanges' barriers
-        rx_regs_dual(v, w, m_hi, A.c, A.s, accb);
-        if (lo_lane >= 0) rx_lane_dual(v, w, lo_lane, A.c, A.s, accb);
+        double sc = A.sc0;
+        rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
+        if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
         // The previous tile's readers of buf are done once every thread is
         // past this tile's first barrier: with the cut barrier (CUT) or the
         // leading barrier of the first exchange.
         if (SC == SC_L021) {
             exchange_dual<0, 2>(v, w, buf, tid, true);
-            rx_regs_dual(v, w, m_lo, A.c, A.s, accb);
+            rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
             exchange_dual<2, 1>(v, w, buf, tid, true);
         } else if (SC == SC_L01) {
             exchange_dual<0, 1>(v, w, buf, tid, true);
         }
         constexpr int LAY = (SC != SC_L0 && !PHI) ? 1 : 0;
         if (SC != SC_L0) {
-            rx_regs_dual(v, w, m_mid, A.c, A.s, accb);
+            rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
             if (LAY == 0) exchange_dual<1, 0>(v, w, buf, tid, true);
         }
         if (PHI) {
             if (SC == SC_L0) __syncthreads();  // kp written by warps 0 and 1
             WT cbase, g0, g1, g2, g3;
             ct.consts(kp, tid, cbase, g0, g1, g2, g3);
+            double tg = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
                               ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
                               ((r & 8) ? g3 : WT(0));
                 const double S = 2.0 * (double)cr - A.W;
-                accg = fma(w[r].x * v[r].y - w[r].y * v[r].x, S, accg);
+                tg = fma(w[r].x * v[r].y - w[r].y * v[r].x, S, tg);
             }
+            accg = fma(sc, tg, accg);
             if (A.scale != 0.0) {
-                const double2 P = phase_of<WT>(A, smtab, cbase);
+                double2 P = phase_of<WT>(A, smtab, cbase);
+                if (INTW) P = make_double2(P.x * A.scale, P.y * A.scale);
                 unphase_base(v, w, P, ct.qtab);
                 unphase_bit(v, w, 0, zpow<WT>(A, smtab, g0));
                 unphase_bit(v, w, 1, zpow<WT>(A, smtab, g1));
