@@ -218,12 +218,12 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per launch of the fused pass kernel from the committed ncu
-    summary (profiles/), or None."""
-    p = os.path.join(ROOT, "profiles", "pass_kernel_n30.md")
+def ncu_traffic_per_launch(kind):
+    """DRAM bytes (read + write) per launch of a pass kind at N=30 from the
+    committed ncu summary (profiles/pass_kernels_n30_p5.md), or None."""
+    p = os.path.join(ROOT, "profiles", "pass_kernels_n30_p5.md")
     try:
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+        m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % kind, open(p).read())
         return float(m.group(1)) if m else None
     except OSError:
         return None
@@ -345,7 +345,9 @@ def run_ours(args):
            "h2d_bytes_per_step": 4 * args.n * args.n, "d2h_bytes_per_step": 8,
            "ms_per_step": 1000.0 * e2e_s / args.steps, "energy_last": energy}
 
-    # ---- roofline of the fused pass kernel (both instances: layer, strided)
+    # ---- roofline.  Dominant kernel: the strided pass (k_pass_tma, two of
+    # the three sweeps of every layer); per_layer: every pass of the layer
+    # (the contiguous phase pass k_pass included).
     peak, peak_src = hbm_peak()
     kern = {}
     tot_ms = tot_b = tot_n = 0
@@ -353,19 +355,25 @@ def run_ours(args):
         if kind in prof:
             kms, kn, kb = prof[kind]
             kern[kind] = {"launches": kn, "ms_avg": kms / kn,
-                          "alg_bytes_per_launch": kb / kn, "gbs": kb / (kms / 1000.0) / 1e9}
+                          "alg_bytes_per_launch": kb / kn, "gbs": kb / (kms / 1000.0) / 1e9,
+                          "frac": kb / (kms / 1000.0) / 1e9 / peak,
+                          "traffic": ncu_traffic_per_launch(kind)}
             tot_ms += kms
             tot_b += kb
             tot_n += kn
-    achieved = tot_b / (tot_ms / 1000.0) / 1e9 if tot_ms else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None,
+    dom = kern.get("strided_pass") or kern.get("layer_pass") or {}
+    layer_gbs = tot_b / (tot_ms / 1000.0) / 1e9 if tot_ms else None
+    roofline = {"bound": "hbm", "achieved": dom.get("gbs"), "peak": peak, "unit": "GB/s",
+                "frac": dom.get("frac"),
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if
                 peak_src == "measured" else "fallback 6.65 TB/s",
-                "traffic": ncu_traffic_per_launch(), "kernel": "fq::k_pass (fused tile pass)",
-                "alg_bytes_per_launch": (tot_b / tot_n) if tot_n else None,
-                "launches": tot_n, "per_kind": kern,
-                "kernel_share_of_step": (tot_ms / ms) if ms else None}
+                "traffic": dom.get("traffic"),
+                "kernel": "fq::k_pass_tma (strided tile pass, TMA pipeline)",
+                "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"),
+                "per_layer": {"gbs": layer_gbs, "frac": layer_gbs / peak if layer_gbs else None,
+                              "launches": tot_n, "kernels": "k_pass (phase pass) + k_pass_tma",
+                              "share_of_step": (tot_ms / ms) if ms else None},
+                "per_kind": kern}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
