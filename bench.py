@@ -448,7 +448,8 @@ def serving_leg(args):
     ss.run_served(forqaoa, sessions[:2], 1, lanes=args.serve_lanes)  # warm-up
     served, wall, stats = ss.run_served(forqaoa, sessions, steps, lanes=args.serve_lanes)
     seq, wall_q = ss.run_sequential(forqaoa, sessions, steps)
-    out = ss.summarize(served, wall, seq, wall_q, stats)
+    plain, wall_p = ss.run_sequential(forqaoa, sessions, steps, reuse=False)
+    out = ss.summarize(served, wall, seq, wall_q, stats, plain, wall_p)
     out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [10, 28], "p": [1, 8],
                      "graph": "G(N,0.5), integer weights 1..10", "seed": 5,
                      "arrivals": "Poisson, mean gap 1 ms", "lanes": args.serve_lanes,

@@ -51,6 +51,7 @@ int prep_graph(const double* upper, int N, GraphPrep& g) {
     FQ_CHECK(N >= 1 && N <= kMaxQubits, FQ_ERR_INVALID, "N=%d out of range [1,%d]", N,
              kMaxQubits);
     g.N = N;
+    g.wabs = 0;
     g.wd.assign((size_t)N * N, 0.0);
     g.wi.assign((size_t)N * N, 0);
     bool integral = true;
@@ -62,6 +63,7 @@ int prep_graph(const double* upper, int N, GraphPrep& g) {
             FQ_CHECK(isfinite(w), FQ_ERR_INVALID, "non-finite weight at (%d,%d)", i, j);
             g.wd[i * N + j] = g.wd[j * N + i] = w;
             W += w;
+            g.wabs += fabs(w);
             if (w != rint(w) || fabs(w) > (double)(1 << 20)) {
                 integral = false;
             } else {

@@ -58,6 +58,7 @@ struct GraphPrep {
     double W = 0;              // sum of weights
     long long cmin = 0, cmax = 0;  // range of cut values (integer path)
     long long gmax = 0;            // max over qubits of sum_v |w_uv| (integer path)
+    double wabs = 0;               // sum of |w| over all edges
 };
 
 int prep_graph(const double* upper, int N, GraphPrep& g);

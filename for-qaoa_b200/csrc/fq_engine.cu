@@ -62,6 +62,37 @@ struct Perm {
     int p[kMaxQubits];
 };
 
+// Per-block max|a-b|^2, max|b|^2, sum|a-b|^2, sum|b|^2 over a grid-stride
+// split (fixed per launch geometry, so the same inputs give the same bits).
+__global__ void k_state_diff(const double2* a, const double2* b, u64 n, double* part) {
+    __shared__ double sh[4][256];
+    double m = 0, mb = 0, s = 0, sb = 0;
+    for (u64 i = blockIdx.x * 256ull + threadIdx.x; i < n; i += (u64)gridDim.x * 256ull) {
+        const double2 x = a[i], y = b[i];
+        const double dx = x.x - y.x, dy = x.y - y.y;
+        const double d2 = dx * dx + dy * dy, b2 = y.x * y.x + y.y * y.y;
+        m = fmax(m, d2);
+        mb = fmax(mb, b2);
+        s += d2;
+        sb += b2;
+    }
+    sh[0][threadIdx.x] = m;
+    sh[1][threadIdx.x] = mb;
+    sh[2][threadIdx.x] = s;
+    sh[3][threadIdx.x] = sb;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sh[0][threadIdx.x] = fmax(sh[0][threadIdx.x], sh[0][threadIdx.x + o]);
+            sh[1][threadIdx.x] = fmax(sh[1][threadIdx.x], sh[1][threadIdx.x + o]);
+            sh[2][threadIdx.x] += sh[2][threadIdx.x + o];
+            sh[3][threadIdx.x] += sh[3][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) part[4 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
 __global__ void k_permute(const double2* __restrict__ src, double2* __restrict__ dst, int N,
                           Perm P) {
     const u64 n = 1ull << N;
@@ -258,6 +289,8 @@ int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma) {
     return FQ_OK;
 }
 
+bool phase_tree_ok(const GraphPrep& g, double gamma) { return fabs(gamma) * g.wabs <= 512.0; }
+
 void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale) {
     A.nhi = engine_nhi(g);
     if (A.nhi > 0) {
@@ -346,6 +379,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
             A.tmask = plan[i].tmask;
             A.gx = gx;
             if (nhi > 0) set_table_args(A, g, gammas[p], scale);
+            A.tree = phase_tree_ok(g, gammas[p]) ? 1 : 0;
             A.gamma = gammas[p];
             A.scale = g.integer ? 1.0 : scale;
             const int ph = i == 0 ? (p == 0 ? PH_INIT : PH_MUL) : PH_NONE;
@@ -584,6 +618,35 @@ int fq_permute_qubits(fq_ctx* ctx, const void* src, void* dst, int N, const int*
     k_permute<<<grid, 256, 0, ctx->stream>>>((const double2*)src, (double2*)dst, N, P);
     FQ_CUDA(cudaGetLastError());
     ctx->launches++;
+    return FQ_OK;
+}
+
+int fq_state_diff(fq_ctx* ctx, const void* a, const void* b, int N, double* out) {
+    FQ_TRY(validate_ctx(ctx));
+    FQ_TRY(check_state((void*)a, N));
+    FQ_TRY(check_state((void*)b, N));
+    FQ_CHECK(out != nullptr, FQ_ERR_INVALID, "null output");
+    const u64 n = 1ull << N;
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)ctx->partial_cap / 4);
+    k_state_diff<<<grid, 256, 0, ctx->stream>>>((const double2*)a, (const double2*)b, n,
+                                                ctx->d_partial);
+    FQ_CUDA(cudaGetLastError());
+    ctx->launches++;
+    std::vector<double> part(4 * (size_t)grid);
+    FQ_CUDA(cudaMemcpyAsync(part.data(), ctx->d_partial, sizeof(double) * part.size(),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    double m = 0, mb = 0, s = 0, sb = 0;
+    for (int i = 0; i < grid; i++) {
+        m = std::max(m, part[4 * i]);
+        mb = std::max(mb, part[4 * i + 1]);
+        s += part[4 * i + 2];
+        sb += part[4 * i + 3];
+    }
+    out[0] = sqrt(m);
+    out[1] = sqrt(mb);
+    out[2] = sqrt(s);
+    out[3] = sqrt(sb);
     return FQ_OK;
 }
 

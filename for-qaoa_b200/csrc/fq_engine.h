@@ -29,6 +29,11 @@ int engine_nhi(const GraphPrep& g);
 // the pass arguments that read it (nhi, dlo, ntab, ph0 = scale*exp(-i*gamma*W/2)).
 int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma);
 void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale);
+// FP64 weights: whether product-tree phases keep the phase arguments within
+// the reference's own rounding (|gamma| * sum|w| small).  Above the bound
+// each amplitude takes sincos of the reference's argument (2C - W)*gamma/2,
+// which is exact for integer-valued weights.
+bool phase_tree_ok(const GraphPrep& g, double gamma);
 int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
 // Fixed-order sum of n partials into one device word.
 int reduce_partials(fq_ctx* ctx, const double* partial, int n, double* out_dev);

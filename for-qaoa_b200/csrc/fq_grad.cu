@@ -190,6 +190,7 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             rotated += __builtin_popcount(plan[i].tmask);
             A.gamma = gammas[k];
             if (nhi > 0) set_table_args(A, g, gammas[k], 1.0);
+            A.tree = phase_tree_ok(g, gammas[k]) ? 1 : 0;
             // Inverse phase (times f^N) only where layers remain.
             A.scale = k > 0 ? pow(f, N) : 0.0;
             const int grid = (int)std::min<i64>(A.ntiles, ctx->num_sms);

@@ -90,6 +90,7 @@ struct PassArgs {
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
     double W;        // total weight
     double scale;    // multiplies the phase
+    int tree;        // FP64 weights: phases by product tree (else one sincos per amplitude)
     double sc0, f2;  // adjoint passes: scale of the inner products at the pass's start, and
                      // the factor (f^2) it gains with every reduced rotation
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
@@ -461,9 +462,10 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     constexpr bool INTW = sizeof(WT) == sizeof(int);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
-    // Product-tree phases: FP64 weights always, integer weights with the
-    // two-level table (nhi == 0 keeps one global-table lookup per amplitude).
-    const bool tree = PH != PH_NONE && (!INTW || A.nhi > 0);
+    // Product-tree phases: integer weights with the two-level table (nhi ==
+    // 0 keeps one global-table lookup per amplitude), FP64 weights when the
+    // host allows it (A.tree: small |gamma| * sum|w|, see phase_tree_ok).
+    const bool tree = PH != PH_NONE && (INTW ? A.nhi > 0 : A.tree != 0);
 
     // ---- set-up: compact weight tables of this pass's tile geometry
     WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
@@ -552,9 +554,17 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                     const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
                                   ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
                                   ((r & 8) ? g3 : WT(0));
-                    const double2 ph = int_phase(A, smtab, (int)cr);
-                    v[r] = (PH == PH_INIT) ? make_double2(ph.x * A.scale, ph.y * A.scale)
-                                           : cmul(v[r], ph);
+                    double2 ph;
+                    if (INTW) {
+                        ph = int_phase(A, smtab, (int)cr);
+                        if (PH == PH_INIT) ph = make_double2(ph.x * A.scale, ph.y * A.scale);
+                    } else {  // the reference's own argument (src/rzz.cu:146-150)
+                        const double S = 2.0 * (double)cr - A.W;
+                        double sn, cs;
+                        sincos(S * A.gamma / 2, &sn, &cs);
+                        ph = make_double2(cs * A.scale, sn * A.scale);
+                    }
+                    v[r] = (PH == PH_INIT) ? ph : cmul(v[r], ph);
                 }
             }
         }

@@ -254,13 +254,33 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             }
             accg = fma(sc, tg, accg);
             if (A.scale != 0.0) {
-                double2 P = phase_of<WT>(A, smtab, cbase);
-                if (INTW) P = make_double2(P.x * A.scale, P.y * A.scale);
-                unphase_base(v, w, P, ct.qtab);
-                unphase_bit(v, w, 0, zpow<WT>(A, smtab, g0));
-                unphase_bit(v, w, 1, zpow<WT>(A, smtab, g1));
-                unphase_bit(v, w, 2, zpow<WT>(A, smtab, g2));
-                unphase_bit(v, w, 3, zpow<WT>(A, smtab, g3));
+                if (INTW ? A.nhi > 0 : A.tree != 0) {  // product tree (see k_pass)
+                    double2 P = phase_of<WT>(A, smtab, cbase);
+                    if (INTW) P = make_double2(P.x * A.scale, P.y * A.scale);
+                    unphase_base(v, w, P, ct.qtab);
+                    unphase_bit(v, w, 0, zpow<WT>(A, smtab, g0));
+                    unphase_bit(v, w, 1, zpow<WT>(A, smtab, g1));
+                    unphase_bit(v, w, 2, zpow<WT>(A, smtab, g2));
+                    unphase_bit(v, w, 3, zpow<WT>(A, smtab, g3));
+                } else {  // one phase per amplitude: global table or sincos
+#pragma unroll
+                    for (int r = 0; r < kRegs; r++) {
+                        const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
+                                      ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
+                                      ((r & 8) ? g3 : WT(0));
+                        double2 ph;
+                        if (INTW) {
+                            ph = int_phase(A, smtab, (int)cr);
+                        } else {
+                            double sn, cs;
+                            sincos((2.0 * (double)cr - A.W) * A.gamma / 2, &sn, &cs);
+                            ph = make_double2(cs, sn);
+                        }
+                        const double2 c = make_double2(ph.x * A.scale, -ph.y * A.scale);
+                        v[r] = cmul(v[r], c);
+                        w[r] = cmul(w[r], c);
+                    }
+                }
             }
         }
         if (ST) {

@@ -66,12 +66,14 @@ struct Session {
 
 struct Lane {
     fq_ctx* ctx = nullptr;
+    cudaStream_t st = nullptr;  // low priority: one-CTA batches go first
     cudaEvent_t done = nullptr;
     bool busy = false;
     Req cur;
 };
 
 constexpr int kBatchCap = 4096;           // small instances per launch
+constexpr int kExpressN = 20;             // lane requests up to this size go first
 constexpr size_t kBatchBytes = 8u << 20;  // descriptors + data per launch
 constexpr int kBatchOut = kBatchCap * (1 + 2 * FQ_SERVE_MAX_LAYERS);
 
@@ -249,15 +251,23 @@ struct fq_server {
         return true;
     }
 
-    // Picks the oldest runnable large request and reserves its session's
-    // buffers (mu held).  Steps of a session keep their order: a request is
-    // skipped if its session is running or an earlier request of the same
-    // session is still queued.
+    // Picks a runnable large request and reserves its session's buffers (mu
+    // held): the oldest with N <= kExpressN if any (short requests are not
+    // queued behind long ones), else the oldest.  Steps of a session keep
+    // their order: a request is skipped if its session is running or an
+    // earlier request of the same session is still queued.
     bool pick_large(Req& out, Session*& sess) {
+        for (int pass = 0; pass < 2; pass++)
+            if (pick_large_if(out, sess, pass == 0 ? kExpressN : kMaxQubits)) return true;
+        return false;
+    }
+
+    bool pick_large_if(Req& out, Session*& sess, int nmax) {
         std::set<uint64_t> blocked;
         for (auto it = large_q.begin(); it != large_q.end(); ++it) {
             if (blocked.count(it->session)) continue;
             blocked.insert(it->session);
+            if (it->N > nmax) continue;
             Session& s = sessions[it->session];
             if (s.busy) continue;
             if (s.sv && s.N != it->N) drop_buffers(s);  // the session changed size
@@ -405,13 +415,19 @@ int fq_server_create(int device, double hbm_budget_bytes, int lanes, fq_server**
     FQ_CHECK(device >= 0 && device < ndev, FQ_ERR_INVALID, "device %d not present (%d)", device,
              ndev);
     FQ_CUDA(cudaSetDevice(device));
+    // Batches of one-CTA instances run at the highest stream priority, so
+    // their CTAs are scheduled ahead of the lanes' pass kernels.
+    int prio_low = 0, prio_high = 0;
+    FQ_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
     fq_server* S = new fq_server();
     S->device = device;
     S->budget = hbm_budget_bytes;
     int st = FQ_OK;
     for (int i = 0; i < lanes && st == FQ_OK; i++) {
         Lane L;
-        st = fq_ctx_create(device, nullptr, &L.ctx);
+        if (cudaStreamCreateWithPriority(&L.st, cudaStreamNonBlocking, prio_low) != cudaSuccess)
+            st = FQ_ERR_CUDA;
+        if (st == FQ_OK) st = fq_ctx_create(device, L.st, &L.ctx);
         if (st == FQ_OK &&
             cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
             st = FQ_ERR_CUDA;
@@ -419,7 +435,7 @@ int fq_server_create(int device, double hbm_budget_bytes, int lanes, fq_server**
     }
     for (auto& B : S->batches) {
         if (st != FQ_OK) break;
-        if (cudaStreamCreateWithFlags(&B.st, cudaStreamNonBlocking) != cudaSuccess ||
+        if (cudaStreamCreateWithPriority(&B.st, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaEventCreateWithFlags(&B.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost(&B.h_in, kBatchBytes) != cudaSuccess ||
             cudaMalloc(&B.d_in, kBatchBytes) != cudaSuccess ||
@@ -464,7 +480,7 @@ int fq_server_destroy(fq_server* S) {
     }
     cudaSetDevice(S->device);
     for (auto& L : S->lanes)
-        if (L.ctx) cudaStreamSynchronize((cudaStream_t)fq_ctx_stream(L.ctx));
+        if (L.st) cudaStreamSynchronize(L.st);
     for (auto& kv : S->sessions) {
         if (kv.second.sv) cudaFreeAsync(kv.second.sv, S->free_stream);
         if (kv.second.cs) cudaFreeAsync(kv.second.cs, S->free_stream);
@@ -477,6 +493,7 @@ int fq_server_destroy(fq_server* S) {
     for (auto& L : S->lanes) {
         if (L.done) cudaEventDestroy(L.done);
         fq_ctx_destroy(L.ctx);
+        if (L.st) cudaStreamDestroy(L.st);
     }
     for (auto& B : S->batches) {
         if (B.st) cudaStreamSynchronize(B.st);

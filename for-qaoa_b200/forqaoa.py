@@ -62,6 +62,7 @@ SIGNATURES = {
     "fq_qaoa_energy_grad": (_i, [_vp, _vp, _vp, _i, _i, _dp, _dp, _dp, _dp, _dp, _dp]),
     "fq_cut_diagonal": (_i, [_vp, _vp, _i, _dp]),
     "fq_permute_qubits": (_i, [_vp, _vp, _vp, _i, _ip]),
+    "fq_state_diff": (_i, [_vp, _vp, _vp, _i, _dp]),
     "fq_reference_label_map": (_i, [_i, _i, _i, _ip]),
     "fq_expectation_noalloc": (_i, [_vp, _i, _dp, _dp, _vp]),
     "fq_server_create": (_i, [_i, _d, _i, ctypes.POINTER(_vp)]),
@@ -322,6 +323,12 @@ class Context:
         p = np.ascontiguousarray(perm, dtype=np.int32)
         _check(_lib.fq_permute_qubits(self.handle, src.ptr, dst.ptr, src.n, _iptr(p)),
                "fq_permute_qubits")
+
+    def state_diff(self, a, b):
+        """{max_abs_diff, max_abs_b, l2_diff, l2_b} of two device states."""
+        out = np.zeros(4)
+        _check(_lib.fq_state_diff(self.handle, a.ptr, b.ptr, a.n, _dptr(out)), "fq_state_diff")
+        return dict(zip(("max_abs_diff", "max_abs_b", "l2_diff", "l2_b"), out.tolist()))
 
     def reference_schedule(self, st, graph, C, gammas, betas):
         """The reference's layer loop (src/Weighted.cpp:97-138) through the

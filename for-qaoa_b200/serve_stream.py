@@ -98,9 +98,10 @@ def run_served(fq, sessions, steps, device=0, lanes=4, budget=150e9):
     return recs, wall, stats
 
 
-def run_sequential(fq, sessions, steps, device=0):
-    """The same evaluations one at a time through fq_qaoa_energy_grad (state
-    and costate allocated once per session)."""
+def run_sequential(fq, sessions, steps, device=0, reuse=True):
+    """The same evaluations one at a time through fq_qaoa_energy_grad.
+    reuse: state and costate allocated once per session; otherwise every
+    call allocates and frees its own (a plain call of the public API)."""
     ctx = fq.Context(device)
     recs = []
     try:
@@ -108,7 +109,7 @@ def run_sequential(fq, sessions, steps, device=0):
         for s in sorted(sessions, key=lambda s: s["arrival"]):
             n = s["N"]
             sv = cs = None
-            if n > 12:
+            if n > 12 and reuse:
                 sv, cs = ctx.state(n), ctx.state(n)
             g, b = s["gammas"].copy(), s["betas"].copy()
             for k in range(steps):
@@ -144,7 +145,7 @@ def compare(served, seq):
     return bad
 
 
-def summarize(served, wall_s, seq=None, wall_q=None, stats=None):
+def summarize(served, wall_s, seq=None, wall_q=None, stats=None, plain=None, wall_p=None):
     out = {"requests": len(served), "evals_per_s": len(served) / wall_s, "wall_s": wall_s,
            "latency_ms_p50": pct([r["latency"] for r in served], 50),
            "latency_ms_p99": pct([r["latency"] for r in served], 99),
@@ -156,6 +157,11 @@ def summarize(served, wall_s, seq=None, wall_q=None, stats=None):
         out["sequential_wall_s"] = wall_q
         out["speedup_vs_sequential"] = out["evals_per_s"] / out["sequential_evals_per_s"]
         out["mismatches_vs_sequential"] = compare(served, seq)
+    if plain is not None:
+        out["plain_evals_per_s"] = len(plain) / wall_p
+        out["plain_wall_s"] = wall_p
+        out["speedup_vs_plain"] = out["evals_per_s"] / out["plain_evals_per_s"]
+        out["mismatches_vs_plain"] = compare(served, plain)
     for lo, hi, name in BUCKETS:
         sr = [r for r in served if lo <= r["N"] <= hi]
         if not sr:
@@ -187,10 +193,11 @@ def main(argv=None):
     sessions, steps = make_stream(a.requests, a.seed, a.steps, a.n_min, a.n_max, a.p_max,
                                   a.gap_ms)
     served, wall, stats = run_served(fq, sessions, steps, 0, a.lanes, a.budget_gb * 1e9)
-    seq = wall_q = None
+    seq = wall_q = plain = wall_p = None
     if not a.no_sequential:
         seq, wall_q = run_sequential(fq, sessions, steps)
-    out = summarize(served, wall, seq, wall_q, stats)
+        plain, wall_p = run_sequential(fq, sessions, steps, reuse=False)
+    out = summarize(served, wall, seq, wall_q, stats, plain, wall_p)
     out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [a.n_min, a.n_max],
                      "p": [1, a.p_max], "graph": "G(N,0.5), integer weights 1..10",
                      "arrivals": f"Poisson, mean gap {a.gap_ms} ms", "seed": a.seed,

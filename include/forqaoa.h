@@ -146,6 +146,11 @@ int fq_expectation(fq_ctx* ctx, const void* sv, int N, const double* graph_upper
 int fq_cut_diagonal(fq_ctx* ctx, void* out, int N, const double* graph_upper);
 /* dst[y] = src[x], y having bit perm[b] equal to bit b of x (out of place). */
 int fq_permute_qubits(fq_ctx* ctx, const void* src, void* dst, int N, const int* perm);
+/* Compares two device states: out[0] = max|a-b|, out[1] = max|b|,
+ * out[2] = ||a-b||_2, out[3] = ||b||_2 (host, synchronises).  For checks of
+ * full-size states without copying them to the host.  No counterpart in the
+ * reference. */
+int fq_state_diff(fq_ctx* ctx, const void* a, const void* b, int N, double* out);
 /* <C> of a device state without allocating any device memory, for callers
  * that cannot call cudaMalloc (their device memory belongs to another
  * allocator, or they cannot afford cudaMalloc's implicit synchronisation).

@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 
 def graph_of(kind, n, rng):
     return {"int": complete_int(n, rng), "fp": gnp_fp(n, rng), "neg": complete_int(n, rng, -5, 5),
-            "sparse": gnp_int(n, rng, 0.3)}[kind]
+            "sparse": gnp_int(n, rng, 0.3), "wide": complete_int(n, rng, 1, 500),
+            "huge": complete_int(n, rng, 1, 5000)}[kind]
 
 
 def check_grad(got, want):
@@ -24,7 +25,7 @@ def check_grad(got, want):
 @pytest.mark.parametrize("n,P,kind", [
     (2, 1, "int"), (4, 3, "fp"), (7, 2, "neg"), (10, 4, "int"), (12, 3, "fp"), (12, 2, "int"),
     (13, 2, "int"), (14, 3, "fp"), (16, 2, "neg"), (17, 3, "sparse"), (20, 2, "int"),
-    (21, 2, "fp"),
+    (21, 2, "fp"), (14, 2, "wide"), (15, 2, "huge"), (10, 2, "wide"),
 ])
 def test_energy_grad_vs_oracle(ctx, oracle, n, P, kind):
     rng = np.random.default_rng(7 * n + P)

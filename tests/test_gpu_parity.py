@@ -10,7 +10,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import (GOLDEN, PKG, ENERGY_RTOL, assert_state_close, complete_int, gnp_fp,
+from conftest import (STATE_RTOL, GOLDEN, PKG, ENERGY_RTOL, assert_state_close, complete_int, gnp_fp,
                       gnp_int, angles)
 
 pytestmark = pytest.mark.gpu
@@ -32,6 +32,12 @@ def graph_of(kind, n, rng):
         return complete_int(n, rng, -5, 5)
     if kind == "sparse":
         return gnp_int(n, rng, 0.2)
+    if kind == "wide":  # integer cut range too wide for the shared two-level table
+        return complete_int(n, rng, 1, 500)
+    if kind == "huge":  # integer weights past the phase table: the FP64 path
+        return complete_int(n, rng, 1, 5000)
+    if kind == "zero":  # no edges: C = 0, only the mixer acts
+        return np.zeros((n, n))
     raise ValueError(kind)
 
 
@@ -194,7 +200,7 @@ def test_fused_engine_vs_golden(ctx, fq, path):
 @pytest.mark.parametrize("n,P,kind", [
     (2, 1, "int"), (3, 2, "fp"), (7, 3, "neg"), (11, 2, "int"), (12, 1, "int"), (12, 3, "fp"),
     (13, 2, "neg"), (16, 4, "int"), (17, 2, "sparse"), (20, 3, "fp"), (21, 2, "int"),
-    (22, 2, "int"),
+    (22, 2, "int"), (14, 2, "wide"), (15, 2, "huge"), (16, 1, "zero"),
 ])
 def test_fused_forward_vs_oracle(ctx, oracle, n, P, kind):
     rng = np.random.default_rng(n * 13 + P)
@@ -312,6 +318,50 @@ def test_engines_agree_n26(ctx, fq):
     finally:
         for s in (a, r, ph):
             s.free()
+
+
+def test_state_diff_matches_host(ctx):
+    rng = np.random.default_rng(5)
+    n = 15
+    a = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    b = a + 1e-9 * (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n))
+    sa, sb = ctx.state(n), ctx.state(n)
+    try:
+        sa.from_host(a)
+        sb.from_host(b)
+        d = ctx.state_diff(sa, sb)
+    finally:
+        sa.free()
+        sb.free()
+    assert d["max_abs_diff"] == pytest.approx(np.abs(a - b).max(), rel=1e-12)
+    assert d["max_abs_b"] == pytest.approx(np.abs(b).max(), rel=1e-12)
+    assert d["l2_diff"] == pytest.approx(np.linalg.norm(a - b), rel=1e-10)
+    assert d["l2_b"] == pytest.approx(np.linalg.norm(b), rel=1e-12)
+
+
+def test_config2_n30_p5_full_state(ctx, fq):
+    """Benchmark config 2 (K_30, integer weights 1..10, p=5, C=12) at full
+    size: the fused engine against the reference schedule (cost sweep, RX
+    chunks of C=12, block swaps) on every one of the 2^30 amplitudes, in one
+    qubit order, compared on the device (1e-12 of max|psi| and relative L2)."""
+    n, P, C = 30, 5, 12
+    rng = np.random.default_rng(30)
+    W = complete_int(n, rng)
+    g, b = angles(rng, P)
+    a, r, ph = ctx.state(n), ctx.state(n), ctx.state(n)
+    try:
+        ea = ctx.qaoa_forward(a, W, g, b)
+        gfin = ctx.reference_schedule(r, W, C, g, b)
+        er = ctx.expectation(r, gfin)
+        lab = fq.reference_label_map(n, C, P)
+        ctx.permute_qubits(a, ph, np.argsort(lab))
+        d = ctx.state_diff(ph, r)
+    finally:
+        for s in (a, r, ph):
+            s.free()
+    assert abs(ea - er) <= ENERGY_RTOL * ea
+    assert d["max_abs_diff"] <= STATE_RTOL * d["max_abs_b"], d
+    assert d["l2_diff"] <= STATE_RTOL * d["l2_b"], d
 
 
 def test_weighted_cli_engines_agree():
