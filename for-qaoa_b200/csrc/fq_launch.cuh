@@ -13,6 +13,7 @@
 #include "fq_ctx.h"
 #include "fq_pass.cuh"
 #include "fq_pass_tma.cuh"
+#include "fq_pass_ws.cuh"
 
 namespace fq {
 
@@ -87,6 +88,18 @@ inline bool tma_for(int ph) {
     return m >= 2 || (m == 1 && ph == PH_NONE);
 }
 
+// FQ_WS=1 runs strided RX passes (no phase, no <C>) as the warp-specialised
+// pipeline with TMA stores (k_pass_ws) instead of k_pass_tma.  Off by
+// default: on B200 at N=30 it measured 4552 GB/s against 4828 GB/s.
+inline bool ws_enabled() {
+    static int m = -1;
+    if (m < 0) {
+        const char* e = getenv("FQ_WS");
+        m = e ? (atoi(e) != 0) : 0;
+    }
+    return m != 0;
+}
+
 // The state as a tensor of float64 whose innermost dimension is one 128-byte
 // row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
 // Returns false for tiles with rows narrower than 8 amplitudes.
@@ -135,8 +148,17 @@ inline int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, Tm
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
     const int tok = prof_begin(ctx);
     bool launched = false;
+    if constexpr (PH == PH_NONE && EX == EX_NONE && GM != GM_NONE) {
+        if (ws_enabled()) {
+            auto fn = k_pass_ws<GM, SC>;
+            FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)ws_pass_smem_bytes()));
+            fn<<<(unsigned)grid, kWsThreads, ws_pass_smem_bytes(), ctx->stream>>>(A, map, G);
+            launched = true;
+        }
+    }
     if constexpr (EX == EX_NONE) {
-        if (tma_mode() == 2) {
+        if (!launched && tma_mode() == 2) {
             auto fn = k_pass_tma2<WT, PH, GM, EX, SC>;
             FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)tma2_pass_smem_bytes<WT>(kMaxQubits)));

@@ -1,8 +1,9 @@
 """GPU parity of every pass variant the engine can select: the per-thread
 load pass (FQ_TMA=0), the default mix (1), the two-group TMA pass (2) and
-the one-group TMA pass for every read-write sweep (3), each with and without
-the L2 prefetch.  The mode is read once per process, so each runs in a
-child process; states and <C> are checked against the oracle."""
+the one-group TMA pass for every read-write sweep (3), with and without the
+L2 prefetch, and the strided passes as the warp-specialised pipeline with
+TMA stores (FQ_WS=1, the default) or the one-group TMA pass (FQ_WS=0).
+The mode is read once per process, so each runs in a child process; states and <C> are checked against the oracle."""
 import json
 import os
 import subprocess
@@ -46,10 +47,11 @@ def cases():
     return out
 
 
-@pytest.mark.parametrize("tma,prefetch", [("0", "0"), ("1", "1"), ("2", "0"), ("3", "1")])
-def test_pass_modes_match_oracle(oracle, tma, prefetch):
+@pytest.mark.parametrize("tma,prefetch,ws", [("0", "0", "1"), ("1", "1", "1"), ("1", "1", "0"),
+                                             ("2", "0", "1"), ("3", "1", "1")])
+def test_pass_modes_match_oracle(oracle, tma, prefetch, ws):
     cs = cases()
-    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch)
+    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws)
     res = subprocess.run([sys.executable, "-c", CHILD % {"pkg": PKG}], input=json.dumps(cs),
                          capture_output=True, text=True, env=env, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
