@@ -199,7 +199,7 @@ int fq_ctx_create(int device, void* stream, fq_ctx** out) {
         cudaDeviceProp prop;
         if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { st = FQ_ERR_CUDA; break; }
         c->num_sms = prop.multiProcessorCount;
-        c->partial_cap = 64 * c->num_sms;
+        c->partial_cap = 256 * c->num_sms;  // room for every pass of a gradient's reverse sweep
         const size_t wbytes = sizeof(double) * kMaxQubits * kMaxQubits;
         if (cudaMalloc(&c->d_w, wbytes) != cudaSuccess ||
             cudaMalloc(&c->d_ptab, sizeof(double2) * kMaxPhaseTable) != cudaSuccess ||

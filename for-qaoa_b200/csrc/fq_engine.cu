@@ -43,6 +43,27 @@ __global__ void k_phase_table2(double2* tab, int dlo, int nhi, double gamma) {
     }
 }
 
+// Tables of k_phase_table2 for up to kMaxTableLayers layers in one launch:
+// layer p's table at tab + p * kTableStride.
+struct LayerGammas {
+    double g[kMaxTableLayers];
+};
+
+__global__ void k_phase_tables2(double2* tab, int dlo, int nhi, LayerGammas lg, int P) {
+    const int p = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    double sn, cs;
+    double2* t = tab + (size_t)p * kTableStride;
+    if (i < kPhaseLo) {
+        sincos(lg.g[p] * (double)i, &sn, &cs);
+        t[i] = make_double2(cs, sn);
+    } else if (i < kPhaseLo + nhi) {
+        sincos(lg.g[p] * (double)(dlo + 32ll * (i - kPhaseLo)), &sn, &cs);
+        t[i] = make_double2(cs, sn);
+    }
+}
+
 // Deterministic sum of n partials into out[0]: fixed strided split and a
 // fixed tree, so the same inputs always give the same bits.
 __global__ void k_reduce_partials(const double* partial, int n, double* out) {
@@ -275,6 +296,23 @@ int engine_nhi(const GraphPrep& g) {
     return nhi <= kPhaseHiMax ? (int)nhi : 0;
 }
 
+int launch_tables2(fq_ctx* ctx, const GraphPrep& g, const double* gammas, int P) {
+    const int nhi = engine_nhi(g);
+    if (nhi == 0 || P > kMaxTableLayers) return FQ_ERR_INVALID;
+    long long dlo, dhi;
+    table_range(g, dlo, dhi);
+    LayerGammas lg;
+    for (int p = 0; p < kMaxTableLayers; p++) lg.g[p] = p < P ? gammas[p] : 0.0;
+    const int n = kPhaseLo + nhi;
+    const int tok = prof_begin(ctx);
+    k_phase_tables2<<<dim3((n + 255) / 256, P), 256, 0, ctx->stream>>>(ctx->d_ptab, (int)dlo, nhi,
+                                                                       lg, P);
+    FQ_CUDA(cudaGetLastError());
+    prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
+    ctx->launches++;
+    return FQ_OK;
+}
+
 int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma) {
     const int nhi = engine_nhi(g);
     if (nhi == 0) return FQ_ERR_INVALID;
@@ -366,11 +404,18 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
         gate_params(betas[p], gm, gx, f);
         const double scale = pow(f, N) * (p == 0 ? amp0 : 1.0);
         const int nhi = g.integer ? engine_nhi(g) : 0;
+        // Two-level tables: all layers' in one launch (layer p's at slot p,
+        // kept for the reverse sweep of a gradient); else one global table
+        // per layer.
+        const bool all_tables = nhi > 0 && P <= kMaxTableLayers;
         if (g.integer) {
-            if (nhi > 0)
+            if (all_tables) {
+                if (p == 0) FQ_TRY(launch_tables2(ctx, g, gammas, P));
+            } else if (nhi > 0) {
                 FQ_TRY(launch_table2(ctx, g, gammas[p]));
-            else
+            } else {
                 FQ_TRY(launch_table(ctx, g, gammas[p], scale));
+            }
         }
         for (size_t i = 0; i < plan.size(); i++) {
             PassArgs A = base_args(ctx, sv, N, g);
@@ -379,6 +424,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
             A.tmask = plan[i].tmask;
             A.gx = gx;
             if (nhi > 0) set_table_args(A, g, gammas[p], scale);
+            if (all_tables) A.ptab = ctx->d_ptab + (size_t)p * kTableStride;
             A.tree = phase_tree_ok(g, gammas[p]) ? 1 : 0;
             A.gamma = gammas[p];
             A.scale = g.integer ? 1.0 : scale;

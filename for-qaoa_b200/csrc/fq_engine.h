@@ -28,6 +28,9 @@ int engine_nhi(const GraphPrep& g);
 // Two-level table of powers of exp(i*gamma) in ctx->d_ptab (nhi > 0), and
 // the pass arguments that read it (nhi, dlo, ntab, ph0 = scale*exp(-i*gamma*W/2)).
 int launch_table2(fq_ctx* ctx, const GraphPrep& g, double gamma);
+// The same for layers 0..P-1 (P <= kMaxTableLayers) in one launch, layer p's
+// table at ctx->d_ptab + p * kTableStride.
+int launch_tables2(fq_ctx* ctx, const GraphPrep& g, const double* gammas, int P);
 void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale);
 // FP64 weights: whether product-tree phases keep the phase arguments within
 // the reference's own rounding (|gamma| * sum|w| small).  Above the bound

@@ -50,6 +50,38 @@ static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, int gm, const Pass
                         : dispatch_dual_gm<GM_COT>(ctx, integer, phi, A, gb, gg);
 }
 
+// One block per reverse pass q (in execution order: layers P-1..0, passes
+// 1..npass-1 then 0): the fixed-order sum of its grid dE/dbeta partials
+// (at part + q * stride) into out[1 + P + k * npass + i] and, for the
+// contiguous pass (i = 0), of its dE/dgamma partials (at + grid) into
+// out[1 + k].
+__global__ void k_reduce_grad(const double* part, int stride, int grid, int P, int npass,
+                              double* out) {
+    __shared__ double sh[2][256];
+    const int q = blockIdx.x;
+    const int k = P - 1 - q / npass, i = (q % npass + 1) % npass;
+    const double* pb = part + (size_t)q * stride;
+    double sb = 0, sg = 0;
+    for (int t = threadIdx.x; t < grid; t += 256) {
+        sb += pb[t];
+        if (i == 0) sg += pb[grid + t];
+    }
+    sh[0][threadIdx.x] = sb;
+    sh[1][threadIdx.x] = sg;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[1 + P + k * npass + i] = sh[0][0];
+        if (i == 0) out[1 + k] = sh[1][0];
+    }
+}
+
 int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream) {
     FQ_CUDA(cudaFuncSetAttribute(k_small_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)small_smem_bytes(kSmallMaxQubits)));
@@ -164,20 +196,27 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
     // with dE/dgamma and the inverse phase.  RX(-beta) runs in reduced form
     // f * G (gate_params): the kernels track the scale the vectors gain
     // (1/f per rotation) and the contiguous pass multiplies f^N back in.
-    double* gb = ctx->d_partial;
+    // Partials of every reverse pass go to their own segment of d_partial
+    // and are summed by one launch at the end (per-pass sums if they do not
+    // fit).  The two-level phase tables of the forward sweep are reused.
+    const int grid = (int)std::min<i64>(1ll << (N - kTileBits), (i64)ctx->num_sms);
+    const int seg = 2 * ctx->num_sms;
+    const bool batched = (i64)P * npass * seg <= ctx->partial_cap;
+    const bool all_tables = g.integer && engine_nhi(g) > 0 && P <= kMaxTableLayers;
+    int q = 0;
     for (int k = P - 1; k >= 0; k--) {
         int gm;
         double gx, f;
         gate_params(-betas[k], gm, gx, f);
         int rotated = 0;  // qubits rotated so far in this layer's reverse sweep
         const int nhi = g.integer ? engine_nhi(g) : 0;
-        if (g.integer) {
+        if (g.integer && !all_tables) {
             if (nhi > 0)
                 FQ_TRY(launch_table2(ctx, g, gammas[k]));
             else
                 FQ_TRY(launch_table(ctx, g, gammas[k], 1.0));
         }
-        for (int o = 1; o <= npass; o++) {
+        for (int o = 1; o <= npass; o++, q++) {
             const int i = o % npass;  // 1, 2, ..., npass-1, then 0
             PassArgs A = base_args(ctx, sv, N, g);
             A.sv2 = (double2*)costate;
@@ -190,15 +229,26 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             rotated += __builtin_popcount(plan[i].tmask);
             A.gamma = gammas[k];
             if (nhi > 0) set_table_args(A, g, gammas[k], 1.0);
+            if (all_tables) A.ptab = ctx->d_ptab + (size_t)k * kTableStride;
             A.tree = phase_tree_ok(g, gammas[k]) ? 1 : 0;
             // Inverse phase (times f^N) only where layers remain.
             A.scale = k > 0 ? pow(f, N) : 0.0;
-            const int grid = (int)std::min<i64>(A.ntiles, ctx->num_sms);
+            double* gb = ctx->d_partial + (batched ? (size_t)q * seg : 0);
             double* gg = gb + grid;
             FQ_TRY(dispatch_dual(ctx, g.integer, i == 0, gm, A, gb, gg));
-            FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + 1 + P + k * npass + i));
-            if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
+            if (!batched) {
+                FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + 1 + P + k * npass + i));
+                if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
+            }
         }
+    }
+    if (batched) {
+        const int tok = prof_begin(ctx);
+        k_reduce_grad<<<P * npass, 256, 0, ctx->stream>>>(ctx->d_partial, seg, grid, P, npass,
+                                                          ctx->d_result);
+        FQ_CUDA(cudaGetLastError());
+        prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
+        ctx->launches++;
     }
     FQ_CUDA(cudaMemcpyAsync(ctx->h_result, ctx->d_result, sizeof(double) * (1 + P + P * npass),
                             cudaMemcpyDeviceToHost, ctx->stream));

@@ -101,6 +101,11 @@ __device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j
 
 constexpr int kPhaseLo = 32;     // low-part entries of the two-level phase table
 constexpr int kPhaseHiMax = 512; // high-part entries kept in shared memory at most
+// Layer tables of the two-level kind built in one launch, kTableStride
+// entries apart in the context's table buffer (kMaxPhaseTable entries).
+constexpr int kTableStride = kPhaseLo + kPhaseHiMax;
+constexpr int kMaxTableLayers = 64;
+static_assert(kTableStride * kMaxTableLayers <= kMaxPhaseTable, "layer tables fit the buffer");
 
 // Shared-memory bytes reserved for the two-level phase table.
 __host__ __device__ inline size_t phase_smem_bytes() {
