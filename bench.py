@@ -13,15 +13,21 @@ Also reported on the same JSON line:
   e2e          the same circuit through the public C ABI with host inputs:
                the graph is uploaded from pinned host memory every step and
                <C> is read back to the host every step;
-  roofline     the fused pass kernel: algorithmic bytes per launch / average
-               launch time (CUDA events on the library's stream), against the
-               measured HBM copy bandwidth;
+  roofline     the dominant kernel (the strided tile pass, k_pass_tma):
+               algorithmic bytes per launch / average launch time (CUDA
+               events on the library's stream), against the measured HBM copy
+               bandwidth; per_layer gives the same over every pass of a layer;
   cpu_baseline the oracle (plain FP64 OpenMP restatement of the reference's
                algorithm) timed on a bounded slice of one layer on the host
                cores, scaled to a full N=30 layer;
   reference_schedule  the reference's own per-layer schedule (cost sweep, RX
                chunks of C=12, block swaps) through this library's per-kernel
                entry points, with per-kernel HBM GB/s;
+  gradient     <C> and its 2p derivatives (adjoint) for K_26, p=10;
+  serving      a sample of the served request stream (sessions of 20
+               energy+gradient steps, N in 10..28, p in 1..8) through the
+               server against the same evaluations as sequential calls, plus
+               the same stream per size class (by_size);
   clocks       SM clock / throttle reasons sampled during the timed region.
 
 `--impl reference` times the reference algorithm on the host cores (the
@@ -454,6 +460,23 @@ def serving_leg(args):
                      "graph": "G(N,0.5), integer weights 1..10", "seed": 5,
                      "arrivals": "Poisson, mean gap 1 ms", "lanes": args.serve_lanes,
                      "budget_gb": 150, "sample_of": "10,000-request stream"}
+    # The same stream restricted to one size class at a time: the mixed
+    # stream's time is dominated by N = 27..28 (HBM-bound one at a time),
+    # these show what batching and overlap do where a request is not.
+    out["by_size"] = {}
+    for lo, hi, n_req, lanes in ((10, 12, 2000, args.serve_lanes), (13, 20, 400, 8),
+                                 (21, 28, 200, args.serve_lanes)):
+        sess, steps = ss.make_stream(n_req, seed=lo, n_min=lo, n_max=hi)
+        sv, w, st = ss.run_served(forqaoa, sess, steps, lanes=lanes)
+        sq, wq = ss.run_sequential(forqaoa, sess, steps)
+        pl, wp = ss.run_sequential(forqaoa, sess, steps, reuse=False)
+        r = ss.summarize(sv, w, sq, wq, None, pl, wp)
+        out["by_size"][f"N {lo}..{hi}"] = {
+            k: r[k] for k in ("requests", "evals_per_s", "latency_ms_p50", "latency_ms_p99",
+                              "sequential_evals_per_s", "speedup_vs_sequential",
+                              "plain_evals_per_s", "speedup_vs_plain",
+                              "mismatches_vs_sequential", "mismatches_vs_plain")}
+        out["by_size"][f"N {lo}..{hi}"]["lanes"] = lanes
     return out
 
 

@@ -61,6 +61,7 @@ struct Session {
     void* cs = nullptr;
     bool busy = false;
     bool closed = false;  // release once the running step completes
+    int queued = 0;       // its requests waiting for a lane
     double last_used = 0;
 };
 
@@ -74,6 +75,7 @@ struct Lane {
 
 constexpr int kBatchCap = 4096;           // small instances per launch
 constexpr int kExpressN = 20;             // lane requests up to this size go first
+constexpr double kEvictIdleS = 0.05;      // a session idle this long may lose its buffers
 constexpr size_t kBatchBytes = 8u << 20;  // descriptors + data per launch
 constexpr int kBatchOut = kBatchCap * (1 + 2 * FQ_SERVE_MAX_LAYERS);
 
@@ -238,11 +240,17 @@ struct fq_server {
 
     // Room for `bytes` more resident bytes: evict idle sessions, least
     // recently used first (mu held).
+    // Only sessions with no step running or queued and idle for kEvictIdleS
+    // are evicted, so a session between two steps of its optimiser loop
+    // keeps its buffers and new sessions wait for room instead of evicting
+    // busy ones (admission by budget, not thrashing).
     bool make_room(size_t bytes) {
+        const double now = now_s();
         while ((double)(used + bytes) > budget) {
             Session* victim = nullptr;
             for (auto& kv : sessions)
-                if (!kv.second.busy && kv.second.sv &&
+                if (!kv.second.busy && kv.second.sv && kv.second.queued == 0 &&
+                    now - kv.second.last_used >= kEvictIdleS &&
                     (!victim || kv.second.last_used < victim->last_used))
                     victim = &kv.second;
             if (!victim) return false;
@@ -257,12 +265,13 @@ struct fq_server {
     // their order: a request is skipped if its session is running or an
     // earlier request of the same session is still queued.
     bool pick_large(Req& out, Session*& sess) {
-        for (int pass = 0; pass < 2; pass++)
-            if (pick_large_if(out, sess, pass == 0 ? kExpressN : kMaxQubits)) return true;
-        return false;
+        return pick_large_if(out, sess, kExpressN, false) ||
+               pick_large_if(out, sess, kMaxQubits, true) ||
+               pick_large_if(out, sess, kMaxQubits, false);
     }
 
-    bool pick_large_if(Req& out, Session*& sess, int nmax) {
+    // resident_only: only sessions whose buffers are already allocated.
+    bool pick_large_if(Req& out, Session*& sess, int nmax, bool resident_only) {
         std::set<uint64_t> blocked;
         for (auto it = large_q.begin(); it != large_q.end(); ++it) {
             if (blocked.count(it->session)) continue;
@@ -270,6 +279,7 @@ struct fq_server {
             if (it->N > nmax) continue;
             Session& s = sessions[it->session];
             if (s.busy) continue;
+            if (resident_only && !(s.sv && s.N == it->N)) continue;
             if (s.sv && s.N != it->N) drop_buffers(s);  // the session changed size
             if (!s.sv) {
                 const size_t bytes = session_bytes(it->N);
@@ -277,8 +287,8 @@ struct fq_server {
                 used += bytes;  // allocated by the lane on its stream
             }
             s.N = it->N;
-            s.closed = false;
             s.busy = true;
+            s.queued--;
             s.last_used = now_s();
             out = std::move(*it);
             large_q.erase(it);
@@ -326,7 +336,7 @@ struct fq_server {
         if (it == sessions.end()) return;
         it->second.busy = false;
         it->second.last_used = now_s();
-        if (it->second.closed) {
+        if (it->second.closed && it->second.queued == 0) {
             drop_buffers(it->second);
             sessions.erase(it);
         }
@@ -542,8 +552,12 @@ int fq_server_submit(fq_server* S, const fq_request* q, uint64_t* ticket) {
     S->in_flight++;
     if (small)
         S->small_q.push_back(std::move(r));
-    else
+    else {
+        Session& ss = S->sessions[r.session];
+        ss.queued++;
+        ss.closed = false;  // new work reopens a closed session
         S->large_q.push_back(std::move(r));
+    }
     S->cv_work.notify_one();
     return FQ_OK;
 }
@@ -571,8 +585,8 @@ int fq_server_close_session(fq_server* S, uint64_t session) {
     std::lock_guard<std::mutex> lk(S->mu);
     auto it = S->sessions.find(session);
     if (it == S->sessions.end()) return FQ_OK;
-    if (it->second.busy) {
-        it->second.closed = true;
+    if (it->second.busy || it->second.queued > 0) {
+        it->second.closed = true;  // released once its queued steps have run
     } else {
         S->drop_buffers(it->second);
         S->sessions.erase(it);

@@ -224,7 +224,8 @@ int fq_server_submit(fq_server* server, const fq_request* request, uint64_t* tic
  * in each result). */
 int fq_server_poll(fq_server* server, fq_result* out, int max_results, int* n_out,
                    int wait_ms);
-/* Releases a session's resident buffers (after its running step, if any). */
+/* Releases a session's resident buffers (after its running and queued steps,
+ * if any). */
 int fq_server_close_session(fq_server* server, uint64_t session);
 int fq_server_stats(fq_server* server, fq_server_counters* counters);
 
