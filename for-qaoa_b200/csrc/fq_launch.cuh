@@ -35,9 +35,9 @@ inline double pass_bytes(int N) {
                 (EX == EX_COSTATE ? 16.0 : 0.0));
 }
 
-template <typename WT, int PH, int GM, int EX, bool ST, int SC>
+template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE>
 inline int launch_ldg(fq_ctx* ctx, const PassArgs& A) {
-    auto fn = k_pass<WT, PH, GM, EX, ST, SC>;
+    auto fn = k_pass<WT, PH, GM, EX, ST, SC, GM2>;
     const size_t smem = pass_smem_bytes<WT>(A.N);
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pass_smem_bytes<WT>(kMaxQubits)));
@@ -233,6 +233,13 @@ int dispatch_rx_tan(fq_ctx* ctx, bool integer, bool energy, const PassArgs& A);
 int dispatch_rx_cot(fq_ctx* ctx, bool integer, bool energy, const PassArgs& A);
 // RX with the full formula of src/rx.cu:47-50 (reference-path kernels).
 int dispatch_rx_full(fq_ctx* ctx, const PassArgs& A);
+// Fused pass: RX (gm1, A.gx) on A.tmask, the next layer's phase, RX (gm2,
+// A.gx2) on A.tmask (k_pass with GM2); one translation unit per weight type.
+int dispatch_fused_int(fq_ctx* ctx, int gm1, int gm2, const PassArgs& A);
+int dispatch_fused_fp(fq_ctx* ctx, int gm1, int gm2, const PassArgs& A);
+inline int dispatch_fused(fq_ctx* ctx, bool integer, int gm1, int gm2, const PassArgs& A) {
+    return integer ? dispatch_fused_int(ctx, gm1, gm2, A) : dispatch_fused_fp(ctx, gm1, gm2, A);
+}
 // Read-only sweeps: <C> partials or the cut diagonal (diag != 0).
 int dispatch_readonly(fq_ctx* ctx, bool integer, bool diag, const PassArgs& A);
 // <C> partials and the costate A.sv2 = C * A.sv.

@@ -38,6 +38,8 @@
 // each amplitude costs a few integer adds.
 #pragma once
 
+#include <type_traits>
+
 #include "fq_common.cuh"
 
 namespace fq {
@@ -86,6 +88,7 @@ struct PassArgs {
     int cmin, ntab, nhi, dlo;
     double ph0x, ph0y;  // ph0 of the two-level table (see ptab)
     double gx;       // t or u of the reduced gate
+    double gx2;      // fused passes (GM2 != GM_NONE): t or u of the next layer's gate
     double c, s;     // cos, sin of angle/2 for GM_FULL
     double gamma;    // FP64 phase path: exp(i*(2C-W)*gamma/2)
     double W;        // total weight
@@ -450,7 +453,12 @@ __device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* sm
     return make_double2(cs * A.scale, sn * A.scale);
 }
 
-template <typename WT, int PH, int GM, int EX, bool ST, int SC>
+// GM2 != GM_NONE makes a fused pass: RX (GM, A.gx) on the tile's targets,
+// then the phase of the next layer (PH_MUL, the tables and angle in A), then
+// that layer's RX (GM2, A.gx2) on the same targets.  With the layer order
+// reversed every other layer, the last pass of one layer and the first of
+// the next share a tile geometry, so two sweeps become one.
+template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE>
 __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
@@ -544,21 +552,22 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             __syncthreads();
             ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }
-        if (PH != PH_NONE) {
+        // The cost phase (PH_INIT writes it, PH_MUL multiplies it in).
+        auto apply_phase = [&](WT cb, WT h0, WT h1, WT h2, WT h3) {
             if (tree) {
-                double2 P = phase_of<WT>(A, smtab, cbase);
+                double2 P = phase_of<WT>(A, smtab, cb);
                 if (INTW && PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
                 phase_base<PH>(v, P, ct.qtab);
-                phase_bit(v, 0, zpow<WT>(A, smtab, g0));
-                phase_bit(v, 1, zpow<WT>(A, smtab, g1));
-                phase_bit(v, 2, zpow<WT>(A, smtab, g2));
-                phase_bit(v, 3, zpow<WT>(A, smtab, g3));
+                phase_bit(v, 0, zpow<WT>(A, smtab, h0));
+                phase_bit(v, 1, zpow<WT>(A, smtab, h1));
+                phase_bit(v, 2, zpow<WT>(A, smtab, h2));
+                phase_bit(v, 3, zpow<WT>(A, smtab, h3));
             } else {
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
-                                  ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
-                                  ((r & 8) ? g3 : WT(0));
+                    const WT cr = cb + ct.creg[r] + ((r & 1) ? h0 : WT(0)) +
+                                  ((r & 2) ? h1 : WT(0)) + ((r & 4) ? h2 : WT(0)) +
+                                  ((r & 8) ? h3 : WT(0));
                     double2 ph;
                     if (INTW) {
                         ph = int_phase(A, smtab, (int)cr);
@@ -572,25 +581,40 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                     v[r] = (PH == PH_INIT) ? ph : cmul(v[r], ph);
                 }
             }
-        }
+        };
+        // RX rounds on the tile's targets, from layout L0 to L1 (or L0 with
+        // SC_L0).  first: the buffer's previous readers are already past a
+        // barrier (the cut barrier), so the first exchange skips its own.
+        auto rx_rounds = [&](auto gm_tag, double gx, bool first) {
+            constexpr int G = decltype(gm_tag)::value;
+            rx_regs<G>(v, m_hi, gx, A.c, A.s);
+            if (lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
+            if (SC == SC_L021) {
+                exchange<0, 2>(v, buf, tid, !(first && CUT));
+                rx_regs<G>(v, m_lo, gx, A.c, A.s);
+                exchange<2, 1>(v, buf, tid, true);
+            } else if (SC == SC_L01) {
+                exchange<0, 1>(v, buf, tid, !(first && CUT));
+            }
+            if (SC != SC_L0) rx_regs<G>(v, m_mid, gx, A.c, A.s);
+        };
+        constexpr bool FUSED = GM2 != GM_NONE;
+        if (PH != PH_NONE && !FUSED) apply_phase(cbase, g0, g1, g2, g3);
         // Final layout: L1 after an exchange, L0 for <C> (the cut
         // decomposition is per L0 slot).
         constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE) ? 1 : 0;
         if (GM != GM_NONE) {
-            rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
-            if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
-            // With the cut barrier above, every thread is past the previous
-            // tile's reads of buf: the first exchange needs no barrier first.
-            if (SC == SC_L021) {
-                exchange<0, 2>(v, buf, tid, !CUT);
-                rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
-                exchange<2, 1>(v, buf, tid, true);
-            } else if (SC == SC_L01) {
-                exchange<0, 1>(v, buf, tid, !CUT);
-            }
-            if (SC != SC_L0) {
-                rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                if (LAY == 0) exchange<1, 0>(v, buf, tid, true);
+            rx_rounds(std::integral_constant<int, GM>(), A.gx, true);
+            if (FUSED) {
+                // Back to L0, where the cut decomposition lives, for the next
+                // layer's phase and rounds.
+                if (SC != SC_L0) exchange<1, 0>(v, buf, tid, true);
+                WT cb, h0, h1, h2, h3;
+                ct.consts(kp, tid, cb, h0, h1, h2, h3);
+                apply_phase(cb, h0, h1, h2, h3);
+                rx_rounds(std::integral_constant<int, FUSED ? GM2 : GM>(), A.gx2, false);
+            } else if (SC != SC_L0 && LAY == 0) {
+                exchange<1, 0>(v, buf, tid, true);
             }
         }
         // The cut constants again for the outputs that need them (read back

@@ -1,8 +1,9 @@
 """GPU parity of every pass variant the engine can select: the per-thread
 load pass (FQ_TMA=0), the default mix (1), the two-group TMA pass (2) and
 the one-group TMA pass for every read-write sweep (3), with and without the
-L2 prefetch, and the strided passes as the warp-specialised pipeline with
-TMA stores (FQ_WS=1, the default) or the one-group TMA pass (FQ_WS=0).
+L2 prefetch, the strided passes as the warp-specialised pipeline with TMA
+stores (FQ_WS=1) or the one-group TMA pass (FQ_WS=0, the default), and the
+fused two-layer schedule (FQ_FUSE=1, the default) or one sweep per pass.
 The mode is read once per process, so each runs in a child process; states and <C> are checked against the oracle."""
 import json
 import os
@@ -47,11 +48,13 @@ def cases():
     return out
 
 
-@pytest.mark.parametrize("tma,prefetch,ws", [("0", "0", "1"), ("1", "1", "1"), ("1", "1", "0"),
-                                             ("2", "0", "1"), ("3", "1", "1")])
-def test_pass_modes_match_oracle(oracle, tma, prefetch, ws):
+@pytest.mark.parametrize("tma,prefetch,ws,fuse", [
+    ("0", "0", "1", "1"), ("1", "1", "1", "1"), ("1", "1", "0", "1"), ("2", "0", "1", "1"),
+    ("3", "1", "1", "1"), ("1", "1", "0", "0"), ("0", "0", "0", "0"),
+])
+def test_pass_modes_match_oracle(oracle, tma, prefetch, ws, fuse):
     cs = cases()
-    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws)
+    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws, FQ_FUSE=fuse)
     res = subprocess.run([sys.executable, "-c", CHILD % {"pkg": PKG}], input=json.dumps(cs),
                          capture_output=True, text=True, env=env, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
