@@ -258,14 +258,14 @@ template <typename WT>
 struct PassSmem {
     static constexpr size_t red = 0;                                // 8 double
     static constexpr size_t ke = red + 8 * sizeof(double);          // 2 x 32 WT
-    static constexpr size_t creg = ke + 64 * sizeof(WT);            // 16 WT
-    static constexpr size_t Dm = creg + 16 * sizeof(WT);            // 24 WT
+    static constexpr size_t creg = ke + 64 * sizeof(WT);            // 2 x 16 WT (L0, L1)
+    static constexpr size_t Dm = creg + 32 * sizeof(WT);            // 24 WT
     static constexpr size_t Ru = Dm + 24 * sizeof(WT);              // 16 WT
     static constexpr size_t wf = Ru + 16 * sizeof(WT);              // kMaxFixed x kWfStride
     static constexpr size_t wu = wf + kMaxFixed * kWfStride * sizeof(WT);  // 12 x kWfStride
-    static constexpr size_t thrc = wu + kTileBits * kWfStride * sizeof(WT);  // 5 x 256 WT
-    static constexpr size_t qtab = (thrc + 5 * kPassThreads * sizeof(WT) + 15) & ~(size_t)15;
-    static constexpr size_t smtab = qtab + 16 * sizeof(double2);
+    static constexpr size_t thrc = wu + kTileBits * kWfStride * sizeof(WT);  // 2 x 5 x 256 WT
+    static constexpr size_t qtab = (thrc + 10 * kPassThreads * sizeof(WT) + 15) & ~(size_t)15;
+    static constexpr size_t smtab = qtab + 32 * sizeof(double2);    // after 2 x 16 qtab
     static constexpr size_t bytes = smtab + sizeof(double2) * (kPhaseLo + kPhaseHiMax);
 };
 
@@ -302,15 +302,16 @@ __device__ __forceinline__ void phase_bit(double2 (&v)[kRegs], int k, double2 E)
 template <typename WT>
 struct CutTables {
     WT* ke;        // 2 x 32, double-buffered per tile: [0] = K, [1+u] = e_u
-    WT* creg;      // 16: cut among the 4 register bits (layout L0)
+    WT* creg;      // 16 per layout (L0, then L1): cut among the 4 register bits
     WT* Dm;        // nF: sum of weights between fixed bit m and the tile bits
     WT* Ru;        // 12: sum of weights between tile bit u and the fixed bits
     WT* wf;        // wf[i * kWfStride + j] = w(fixed i, fixed j)
     WT* wu;        // wu[u * kWfStride + j] = w(tile u, fixed j)
-    WT* thrc;      // 5 x 256 per-thread constants: [0] cut among the thread's
-                   // 8 tile bits (plus their edges to set register bits),
-                   // [1+k] = f_k, the thread's part of g_k
-    double2* qtab; // 16: z^creg[r], z = exp(i*gamma) (phase passes)
+    WT* thrc;      // 5 x 256 per-thread constants per layout (L0, then L1):
+                   // [0] cut among the thread's 8 tile bits (plus their
+                   // edges to set register bits), [1+k] = f_k, the thread's
+                   // part of g_k
+    double2* qtab; // 16 per layout: z^creg[r], z = exp(i*gamma) (phase passes)
 
     __device__ CutTables(unsigned char* sm) {
         using SM = PassSmem<WT>;
@@ -347,48 +348,52 @@ struct CutTables {
             WT r = 0;
             for (int i = 0; i < nF; i++) r += sw[u * N + fixed_phys(i, l, a)];
             Ru[tid - 32] = r;
-        } else if (tid >= 64 && tid < 80) {
-            const int r = tid - 64;
+        } else if (tid >= 64 && tid < 96) {
+            const int L = (tid - 64) >> 4, r = tid & 15;
             WT c = 0;
             for (int k = 0; k < 4; k++)
                 for (int k2 = k + 1; k2 < 4; k2++)
                     if (((r >> k) ^ (r >> k2)) & 1)
-                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
-            creg[r] = c;
+                        c += sw[tile_phys(rbit(L, k), l, a) * N + tile_phys(rbit(L, k2), l, a)];
+            creg[16 * L + r] = c;
             if (QT) {
                 double sn, cs;
                 sincos(gamma * (double)c, &sn, &cs);
-                qtab[r] = make_double2(cs, sn);
+                qtab[16 * L + r] = make_double2(cs, sn);
             }
         }
-        WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
-        for (int j = 0; j < 8; j++) {
-            const int pj = tile_phys(j, l, a);
-            const int tj = (tid >> j) & 1;
-            for (int j2 = j + 1; j2 < 8; j2++)
-                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
-            // Edge (j, 8+k) is cut iff t_j != r_k: t_j + r_k (1 - 2 t_j).
-            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
-            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
-            if (tj) {
-                athr += w0 + w1 + w2 + w3;
-                f0 -= w0;
-                f1 -= w1;
-                f2 -= w2;
-                f3 -= w3;
-            } else {
-                f0 += w0;
-                f1 += w1;
-                f2 += w2;
-                f3 += w3;
+        for (int L = 0; L < 2; L++) {
+            const int T = L == 0 ? tid : lay_index<1>(tid, 0);  // slot 0's tile index
+            WT athr = 0, f[4] = {0, 0, 0, 0};
+            for (int j = 0; j < 8; j++) {
+                const int pj = tile_phys(tbit(L, j), l, a);
+                const int tj = (T >> tbit(L, j)) & 1;
+                for (int j2 = j + 1; j2 < 8; j2++)
+                    if (tj ^ ((T >> tbit(L, j2)) & 1))
+                        athr += sw[pj * N + tile_phys(tbit(L, j2), l, a)];
+                // Edge (thread bit j, register bit k) is cut iff t_j != r_k:
+                // t_j + r_k (1 - 2 t_j).
+                for (int k = 0; k < 4; k++) {
+                    const WT w = sw[pj * N + tile_phys(rbit(L, k), l, a)];
+                    if (tj) {
+                        athr += w;
+                        f[k] -= w;
+                    } else {
+                        f[k] += w;
+                    }
+                }
             }
+            WT* tc = thrc + 5 * kPassThreads * L;
+            tc[tid] = athr;
+            for (int k = 0; k < 4; k++) tc[(1 + k) * kPassThreads + tid] = f[k];
         }
-        thrc[tid] = athr;
-        thrc[kPassThreads + tid] = f0;
-        thrc[2 * kPassThreads + tid] = f1;
-        thrc[3 * kPassThreads + tid] = f2;
-        thrc[4 * kPassThreads + tid] = f3;
     }
+
+    // Tile bit of register bit k and of thread bit j in layout L (L0: the
+    // thread's bits are tile bits 0..7, registers 8..11; L1: thread bits
+    // 0..3 and 8..11, registers 4..7).
+    __host__ __device__ static int rbit(int L, int k) { return L == 0 ? 8 + k : 4 + k; }
+    __host__ __device__ static int tbit(int L, int j) { return L == 0 ? j : (j < 4 ? j : j + 4); }
 
     // K and e_u of the tile at `base` into kp (warps 0 and 1 of the block;
     // the caller synchronises before reading kp).
@@ -421,15 +426,18 @@ struct CutTables {
     // cb = cut value of the thread's register slot 0, g_k = change of the
     // cut when register bit k is set; slot r has c_r = cb + creg[r] +
     // sum_k r_k g_k.
+    template <int L = 0>
     __device__ void consts(const WT* kp, int tid, WT& cb, WT& g0, WT& g1, WT& g2, WT& g3) const {
-        cb = kp[0] + thrc[tid];
+        const WT* tc = thrc + 5 * kPassThreads * L;
+        const int T = L == 0 ? tid : lay_index<1>(tid, 0);
+        cb = kp[0] + tc[tid];
 #pragma unroll
         for (int j = 0; j < 8; j++)
-            if ((tid >> j) & 1) cb += kp[1 + j];
-        g0 = thrc[kPassThreads + tid] + kp[9];
-        g1 = thrc[2 * kPassThreads + tid] + kp[10];
-        g2 = thrc[3 * kPassThreads + tid] + kp[11];
-        g3 = thrc[4 * kPassThreads + tid] + kp[12];
+            if ((T >> tbit(L, j)) & 1) cb += kp[1 + tbit(L, j)];
+        g0 = tc[kPassThreads + tid] + kp[1 + rbit(L, 0)];
+        g1 = tc[2 * kPassThreads + tid] + kp[1 + rbit(L, 1)];
+        g2 = tc[3 * kPassThreads + tid] + kp[1 + rbit(L, 2)];
+        g3 = tc[4 * kPassThreads + tid] + kp[1 + rbit(L, 3)];
     }
 };
 
@@ -552,12 +560,16 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             __syncthreads();
             ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }
-        // The cost phase (PH_INIT writes it, PH_MUL multiplies it in).
-        auto apply_phase = [&](WT cb, WT h0, WT h1, WT h2, WT h3) {
+        // The cost phase (PH_INIT writes it, PH_MUL multiplies it in), with
+        // the registers in layout LL (0 or 1) and that layout's constants.
+        auto apply_phase = [&](auto lay_tag, WT cb, WT h0, WT h1, WT h2, WT h3) {
+            constexpr int LL = decltype(lay_tag)::value;
+            const double2* qt = ct.qtab + 16 * LL;
+            const WT* crg = ct.creg + 16 * LL;
             if (tree) {
                 double2 P = phase_of<WT>(A, smtab, cb);
                 if (INTW && PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
-                phase_base<PH>(v, P, ct.qtab);
+                phase_base<PH>(v, P, qt);
                 phase_bit(v, 0, zpow<WT>(A, smtab, h0));
                 phase_bit(v, 1, zpow<WT>(A, smtab, h1));
                 phase_bit(v, 2, zpow<WT>(A, smtab, h2));
@@ -565,7 +577,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             } else {
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    const WT cr = cb + ct.creg[r] + ((r & 1) ? h0 : WT(0)) +
+                    const WT cr = cb + crg[r] + ((r & 1) ? h0 : WT(0)) +
                                   ((r & 2) ? h1 : WT(0)) + ((r & 4) ? h2 : WT(0)) +
                                   ((r & 8) ? h3 : WT(0));
                     double2 ph;
@@ -599,20 +611,40 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             if (SC != SC_L0) rx_regs<G>(v, m_mid, gx, A.c, A.s);
         };
         constexpr bool FUSED = GM2 != GM_NONE;
-        if (PH != PH_NONE && !FUSED) apply_phase(cbase, g0, g1, g2, g3);
+        using L0t = std::integral_constant<int, 0>;
+        using L1t = std::integral_constant<int, 1>;
+        if (PH != PH_NONE && !FUSED) apply_phase(L0t(), cbase, g0, g1, g2, g3);
         // Final layout: L1 after an exchange, L0 for <C> (the cut
-        // decomposition is per L0 slot).
-        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE) ? 1 : 0;
+        // decomposition is per L0 slot) and for fused passes (their second
+        // rounds run back from L1 to L0).
+        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE && !FUSED) ? 1 : 0;
         if (GM != GM_NONE) {
             rx_rounds(std::integral_constant<int, GM>(), A.gx, true);
             if (FUSED) {
-                // Back to L0, where the cut decomposition lives, for the next
-                // layer's phase and rounds.
-                if (SC != SC_L0) exchange<1, 0>(v, buf, tid, true);
+                constexpr int G2 = FUSED ? GM2 : GM;
                 WT cb, h0, h1, h2, h3;
-                ct.consts(kp, tid, cb, h0, h1, h2, h3);
-                apply_phase(cb, h0, h1, h2, h3);
-                rx_rounds(std::integral_constant<int, FUSED ? GM2 : GM>(), A.gx2, false);
+                if (SC == SC_L0) {
+                    ct.consts(kp, tid, cb, h0, h1, h2, h3);
+                    apply_phase(L0t(), cb, h0, h1, h2, h3);
+                    rx_rounds(std::integral_constant<int, G2>(), A.gx2, false);
+                } else {
+                    // The next layer's phase in L1, then its rounds in the
+                    // opposite order: L1 -> (L2 ->) L0.
+                    ct.template consts<1>(kp, tid, cb, h0, h1, h2, h3);
+                    apply_phase(L1t(), cb, h0, h1, h2, h3);
+                    rx_regs<G2>(v, m_mid, A.gx2, A.c, A.s);
+                    // A single target among tile bits 0..3 is a lane bit in L1
+                    // as in L0.
+                    if (lo_lane >= 0) rx_lane<G2>(v, lo_lane, A.gx2, A.c, A.s);
+                    if (SC == SC_L021) {
+                        exchange<1, 2>(v, buf, tid, true);
+                        rx_regs<G2>(v, m_lo, A.gx2, A.c, A.s);
+                        exchange<2, 0>(v, buf, tid, true);
+                    } else {
+                        exchange<1, 0>(v, buf, tid, true);
+                    }
+                    rx_regs<G2>(v, m_hi, A.gx2, A.c, A.s);
+                }
             } else if (SC != SC_L0 && LAY == 0) {
                 exchange<1, 0>(v, buf, tid, true);
             }
