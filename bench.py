@@ -377,7 +377,10 @@ def run_ours(args):
                 "kernel": "fq::k_pass_tma (strided tile pass, TMA pipeline)",
                 "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"),
                 "per_layer": {"gbs": layer_gbs, "frac": layer_gbs / peak if layer_gbs else None,
-                              "launches": tot_n, "kernels": "k_pass (phase pass) + k_pass_tma",
+                              "launches": tot_n,
+                              "kernels": "k_pass (phase and fused passes) + k_pass_tma",
+                              "sweeps_per_layer": tot_n / (args.steps * args.p),
+                              "alg_bytes_per_layer": tot_b / (args.steps * args.p),
                               "share_of_step": (tot_ms / ms) if ms else None},
                 "per_kind": kern}
 
