@@ -13,7 +13,11 @@
 //   --seed S                  seed of the generators (default 1)
 //   --expect                  print <C>
 //   --dump FILE               write the final state (raw complex128) in the
-//                             reference's physical qubit order
+//                             reference's physical qubit order, and beside it
+//                             FILE.labels: the logical qubit at each physical
+//                             bit position, and FILE.circuit: N P, gammas,
+//                             betas, the N x N graph (validate_dump.py reads
+//                             all three)
 // Timing uses CUDA events around the layer loop, after a device sync, so it
 // covers the GPU work (the reference's non-MPI timer stops before its sync,
 // src/Weighted.cpp:140-150).
@@ -215,6 +219,24 @@ int main(int argc, char* argv[]) {
             if (!f) throw fq::Error(FQ_ERR_INVALID, "cannot open " + dump);
             fwrite(qureg.hState, sizeof(Complex), 1ull << N, f);
             fclose(f);
+            // Sidecar: the reference's physical -> logical label map after P
+            // layers with chunk C (src/Weighted.cpp:97-138 never undoes it).
+            std::vector<int> refl(N);
+            fq_reference_label_map(N, C, P, refl.data());
+            FILE* fl = fopen((dump + ".labels").c_str(), "w");
+            if (!fl) throw fq::Error(FQ_ERR_INVALID, "cannot open " + dump + ".labels");
+            for (int b = 0; b < N; b++) fprintf(fl, "%d%c", refl[b], b + 1 < N ? ' ' : '\n');
+            fclose(fl);
+            // Sidecar: the circuit (N P, gammas, betas, the N x N logical graph).
+            FILE* fc = fopen((dump + ".circuit").c_str(), "w");
+            if (!fc) throw fq::Error(FQ_ERR_INVALID, "cannot open " + dump + ".circuit");
+            fprintf(fc, "%d %d\n", N, P);
+            for (int p = 0; p < P; p++) fprintf(fc, "%.17g%c", gam[p], p + 1 < P ? ' ' : '\n');
+            for (int p = 0; p < P; p++) fprintf(fc, "%.17g%c", bet[p], p + 1 < P ? ' ' : '\n');
+            for (int i = 0; i < N; i++)
+                for (int j = 0; j < N; j++)
+                    fprintf(fc, "%.17g%c", j > i ? g0[i * N + j] : 0.0, j + 1 < N ? ' ' : '\n');
+            fclose(fc);
         }
         fflush(stdout);
         free2DGraph(graph);

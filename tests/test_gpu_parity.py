@@ -5,6 +5,7 @@ size-independent properties."""
 import glob
 import os
 import subprocess
+import sys
 import tempfile
 
 import numpy as np
@@ -379,6 +380,24 @@ def test_weighted_cli_engines_agree():
             outs.append(np.fromfile(f, dtype=np.complex128))
         assert_state_close(outs[1], outs[0], what="CLI fused vs reference")
         assert abs(es[0] - es[1]) <= ENERGY_RTOL * es[0]
+
+
+@pytest.mark.parametrize("engine", ["fused", "reference"])
+def test_weighted_cli_dump_validates(engine):
+    """The CLI's dump with its label-map and circuit sidecars passes the
+    independent dense check (validate_dump.py), for a weighted graph whose
+    state does change under a wrong relabelling."""
+    exe = os.path.join(PKG, "weighted")
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "s.bin")
+        r = subprocess.run([exe, "3", "13", "0", "5", "13", "--engine", engine, "--weights",
+                            "int", "--angles", "random", "--seed", "7", "--dump", f],
+                           capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr
+        v = subprocess.run([sys.executable, os.path.join(PKG, "validate_dump.py"), f, "13", "3",
+                            "--tol", "1e-12"], capture_output=True, text=True, timeout=300)
+        assert v.returncode == 0, v.stdout + v.stderr
+        assert v.stdout.startswith("PASS")
 
 
 def test_weighted_cli_rejects_multi_device():
