@@ -405,3 +405,39 @@ def test_weighted_cli_rejects_multi_device():
     r = subprocess.run([exe, "1", "12", "1", "4", "8"], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode == 1 and "D=1" in r.stderr
+
+
+def test_refapi_unweighted_bitmask_path(fq, oracle, tmp_path):
+    """A program written against the reference-style C++ API only
+    (tests/refapi_unweighted.cpp, compiled here against include/refapi and
+    libforqaoa.so) runs the reference's layer loop on an unweighted graph of
+    64-bit neighbour masks; its state, mapped through the reference's label
+    map, matches the oracle on the same unit-weight graph."""
+    import shutil
+    cxx = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    exe = tmp_path / "refapi_unweighted"
+    here = os.path.dirname(os.path.abspath(__file__))
+    inc = os.path.join(os.path.dirname(here), "include")
+    r = subprocess.run([cxx, "-std=c++17", "-I", inc, os.path.join(here, "refapi_unweighted.cpp"),
+                        "-L", PKG, "-lforqaoa", "-Xlinker", "-rpath=" + PKG, "-o", str(exe)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    N, P, C = 14, 2, 5
+    out = tmp_path / "s.bin"
+    r = subprocess.run([str(exe), str(P), str(N), str(C), "11", str(out)], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    W = np.zeros((N, N))
+    for line in open(str(out) + ".edges"):
+        i, j = map(int, line.split())
+        W[i, j] = 1.0
+    want = oracle.qaoa_logical(W, np.full(P, 0.7), np.full(P, 0.45))
+    phys = np.fromfile(out, dtype=np.complex128)
+    lab = fq.reference_label_map(N, C, P)
+    y = np.arange(1 << N)
+    x = np.zeros_like(y)
+    for b, q in enumerate(lab):
+        x |= ((y >> b) & 1) << int(q)
+    got = np.empty_like(phys)
+    got[x] = phys
+    assert_state_close(got, want, what="C++ API, unweighted graph")
