@@ -227,13 +227,27 @@ __device__ __forceinline__ void exchange_g(double2 (&v)[kRegs], double2* buf, in
     for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(gtid, r))];
 }
 
+// Layouts L1 and L2 both put tile bits 9..11 on the warp index, so a change
+// between them stays inside each warp's 512-amplitude region of buf (the
+// swizzle only permutes bits 0..2): a warp barrier is enough.  Such an
+// exchange must follow reads of buf in L1 or L2 (the warp's own region), as
+// every schedule here does; exchanges from or to L0 cross warps and use the
+// block barrier.
+template <int LF, int LT>
+__device__ __forceinline__ void buf_sync() {
+    if (LF != 0 && LT != 0)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
 template <int LF, int LT>
 __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid,
                                          bool wait_readers = true) {
-    if (wait_readers) __syncthreads();  // previous readers of buf are done
+    if (wait_readers) buf_sync<LF, LT>();  // previous readers of buf are done
 #pragma unroll
     for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
-    __syncthreads();
+    buf_sync<LF, LT>();
 #pragma unroll
     for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
 }

@@ -87,14 +87,14 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
 template <int LF, int LT>
 __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[kRegs],
                                               double2* buf, int tid, bool wait_readers = true) {
-    if (wait_readers) __syncthreads();  // previous readers of buf are done
+    if (wait_readers) buf_sync<LF, LT>();  // previous readers of buf are done
 #pragma unroll
     for (int r = 0; r < kRegs; r++) {
         const int sl = xslot(lay_index<LF>(tid, r));
         buf[sl] = v[r];
         buf[kTile + sl] = w[r];
     }
-    __syncthreads();
+    buf_sync<LF, LT>();
 #pragma unroll
     for (int r = 0; r < kRegs; r++) {
         const int sl = xslot(lay_index<LT>(tid, r));
