@@ -527,7 +527,6 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     auto off1 = [&](int r) -> i64 {
         return ((r & 1) ? s4 : 0) + ((r & 2) ? s5 : 0) + ((r & 4) ? s6 : 0) + ((r & 8) ? s7 : 0);
     };
-    const int pf_step = l < 3 ? l : 3;  // prefetch granularity: 128-byte lines or rows
     const bool contiguous = (l == kTileBits);
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     // Tile bits 0..3: two or more targets take a register round in L2
@@ -547,24 +546,18 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             if (LOAD) v[r] = __ldcs(p + off0(r));
             else v[r] = make_double2(0.0, 0.0);
         }
-        if (LOAD && A.pf_dist > 0) {
-            // Stream this CTA's tile pf_dist strides ahead from HBM into L2.
+        if (LOAD && A.pf_dist > 0 && contiguous) {
+            // Stream this CTA's tile pf_dist strides ahead from HBM into L2
+            // (one bulk prefetch).  Strided tiles are not prefetched: the
+            // per-row prefetches cost more than they saved (measured on the
+            // fused strided pass: 12.2 ms with, 11.2 ms without).
             const i64 T2 = T + (i64)A.pf_dist * gridDim.x;
-            if (T2 < A.ntiles) {
+            if (T2 < A.ntiles && tid == 0) {
                 const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
                                ((T2 >> nmid) << (a + kTileBits - l));
-                if (contiguous) {
-                    if (tid == 0)
-                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
-                                     "r"((unsigned)(kTile * sizeof(double2)))
-                                     : "memory");
-                } else {
-                    for (int j = tid; j < (1 << (kTileBits - pf_step)); j += kPassThreads) {
-                        const int t = j << pf_step;
-                        asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + b2 + tile_off(t, l, a))
-                                     : "memory");
-                    }
-                }
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
+                             "r"((unsigned)(kTile * sizeof(double2)))
+                             : "memory");
             }
         }
         WT* const kp = ct.ke + 32 * par;  // double-buffered: no barrier for the previous readers
