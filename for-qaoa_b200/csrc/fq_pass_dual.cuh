@@ -13,8 +13,9 @@
 // A backward layer is the forward layer's passes over (psi, lambda): the
 // strided passes undo RX on their qubits, then the contiguous pass undoes RX
 // on qubits 0..11, accumulates dE/dgamma_k and applies the inverse phase.
-// The pass uses the full RX formula (src/rx.cu:47-50) with -beta, so the
-// inner products are taken on exactly scaled vectors.
+// RX(-beta) runs in the reduced form of the forward engine; the kernel
+// tracks the scale that gives the vectors and corrects every inner product
+// for it, and the inverse phase restores the true scale.
 //
 // 256 threads x 16 amplitudes x 2 vectors in registers, one CTA per SM; the
 // layouts, exchanges (one 64 KB buffer per vector) and cut decomposition are
@@ -108,30 +109,6 @@ __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[
 template <typename WT>
 __host__ __device__ inline size_t dual_smem_bytes(int) {
     return 2 * sizeof(double2) * kTile + PassSmem<WT>::bytes + 16 * sizeof(double);
-}
-
-// v *= conj(P * Q_r) on every slot, then conj(E) on the slots with bit k:
-// the inverse of the phase applied by k_pass (see phase_base / phase_bit).
-__device__ __forceinline__ void unphase_base(double2 (&v)[kRegs], double2 (&w)[kRegs], double2 P,
-                                             const double2* qtab) {
-#pragma unroll
-    for (int r = 0; r < kRegs; r++) {
-        const double2 ph = cmul(P, qtab[r]);
-        const double2 c = make_double2(ph.x, -ph.y);
-        v[r] = cmul(v[r], c);
-        w[r] = cmul(w[r], c);
-    }
-}
-
-__device__ __forceinline__ void unphase_bit(double2 (&v)[kRegs], double2 (&w)[kRegs], int k,
-                                            double2 E) {
-    const double2 c = make_double2(E.x, -E.y);
-#pragma unroll
-    for (int r = 0; r < kRegs; r++)
-        if ((r >> k) & 1) {
-            v[r] = cmul(v[r], c);
-            w[r] = cmul(w[r], c);
-        }
 }
 
 // RX(-beta) in reduced form GM (A.gx = t or u, A.f2 = f^2, A.sc0 = scale of
@@ -257,11 +234,22 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 if (INTW ? A.nhi > 0 : A.tree != 0) {  // product tree (see k_pass)
                     double2 P = phase_of<WT>(A, smtab, cbase);
                     if (INTW) P = make_double2(P.x * A.scale, P.y * A.scale);
-                    unphase_base(v, w, P, ct.qtab);
-                    unphase_bit(v, w, 0, zpow<WT>(A, smtab, g0));
-                    unphase_bit(v, w, 1, zpow<WT>(A, smtab, g1));
-                    unphase_bit(v, w, 2, zpow<WT>(A, smtab, g2));
-                    unphase_bit(v, w, 3, zpow<WT>(A, smtab, g3));
+                    // Registers are plentiful here (one CTA per SM): build
+                    // every slot's phase once from L = P * {1, E0, E1, E0 E1}
+                    // and H = {1, E2, E3, E2 E3} and apply its conjugate to
+                    // both vectors.
+                    const double2 E0 = zpow<WT>(A, smtab, g0), E1 = zpow<WT>(A, smtab, g1);
+                    const double2 E2 = zpow<WT>(A, smtab, g2), E3 = zpow<WT>(A, smtab, g3);
+                    const double2 L[4] = {P, cmul(P, E0), cmul(P, E1), cmul(cmul(P, E0), E1)};
+                    const double2 H[4] = {make_double2(1.0, 0.0), E2, E3, cmul(E2, E3)};
+#pragma unroll
+                    for (int r = 0; r < kRegs; r++) {
+                        double2 ph = cmul(L[r & 3], ct.qtab[r]);
+                        if (r >> 2) ph = cmul(ph, H[r >> 2]);
+                        const double2 c = make_double2(ph.x, -ph.y);
+                        v[r] = cmul(v[r], c);
+                        w[r] = cmul(w[r], c);
+                    }
                 } else {  // one phase per amplitude: global table or sincos
 #pragma unroll
                     for (int r = 0; r < kRegs; r++) {
