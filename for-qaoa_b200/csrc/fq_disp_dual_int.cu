@@ -1,0 +1,11 @@
+// fq_disp_dual_int.cu -- adjoint phase passes (plain and fused), integer weights.
+#include "fq_disp_dual.cuh"
+
+namespace fq {
+
+int dispatch_dual_phase_int(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
+                            double* gg, double* gb2) {
+    return dual_phase_dispatch<int>(ctx, gm, gm2, A, gb, gg, gb2);
+}
+
+}  // namespace fq

@@ -391,11 +391,7 @@ int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g) {
     return FQ_OK;
 }
 
-// The fused forward circuit for N >= 12 (see fq_qaoa_forward); with energy
-// != NULL the last sweep also sums <C> and *energy receives it.
-// FQ_FUSE=0 turns the fused two-layer schedule off (one sweep per pass of
-// every layer, as measured before it).
-static bool fuse_enabled() {
+bool fuse_enabled() {
     static int m = -1;
     if (m < 0) {
         const char* e = getenv("FQ_FUSE");
@@ -403,6 +399,9 @@ static bool fuse_enabled() {
     }
     return m != 0;
 }
+
+// The fused forward circuit for N >= 12 (see fq_qaoa_forward); with energy
+// != NULL the last sweep also sums <C> and *energy receives it.
 
 // The fused schedule: layer p visits its passes in plan order when p is even
 // and in reverse order when p is odd, so the last pass of layer p and the

@@ -38,6 +38,10 @@ void set_table_args(PassArgs& A, const GraphPrep& g, double gamma, double scale)
 // which is exact for integer-valued weights.
 bool phase_tree_ok(const GraphPrep& g, double gamma);
 int launch_table(fq_ctx* ctx, const GraphPrep& g, double gamma, double scale);
+// Whether the fused two-layer schedules run (the forward circuit's and the
+// gradient's reverse sweep); FQ_FUSE=0 turns them off (one sweep per pass of
+// every layer).
+bool fuse_enabled();
 // Fixed-order sum of n partials into one device word.
 int reduce_partials(fq_ctx* ctx, const double* partial, int n, double* out_dev);
 int reduce_to_result(fq_ctx* ctx, int n);

@@ -10,76 +10,41 @@
 #include "fq_ctx.h"
 #include "fq_engine.h"
 #include "fq_launch.cuh"
-#include "fq_pass_dual.cuh"
+#include "fq_disp_dual.cuh"
 #include "fq_small.cuh"
 
 namespace fq {
 
-template <typename WT, bool PHI, int SC, int GM>
-static int launch_dual(fq_ctx* ctx, const PassArgs& A, double* gb, double* gg) {
-    auto fn = k_pass_dual<WT, PHI, SC, true, GM>;
-    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)dual_smem_bytes<WT>(kMaxQubits)));
-    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
-    const int tok = prof_begin(ctx);
-    fn<<<(unsigned)grid, kPassThreads, dual_smem_bytes<WT>(A.N), ctx->stream>>>(A, gb, gg);
-    FQ_CUDA(cudaGetLastError());
-    prof_end(ctx, tok, FQ_KIND_ADJOINT, 64.0 * (double)(1ull << A.N));
-    ctx->launches++;
-    return FQ_OK;
+// RX(-beta) on A.tmask alone (the weights are not read: one instance).
+static int dispatch_dual_rx(fq_ctx* ctx, int gm, const PassArgs& A, double* gb) {
+    FQ_CHECK(gm == GM_TAN || gm == GM_COT, FQ_ERR_INVALID, "adjoint pass gate mode %d", gm);
+    return gm == GM_TAN ? dual_sc<int, false, GM_TAN, GM_NONE>(ctx, A, gb, nullptr, nullptr)
+                        : dual_sc<int, false, GM_COT, GM_NONE>(ctx, A, gb, nullptr, nullptr);
 }
 
-template <int GM>
-static int dispatch_dual_gm(fq_ctx* ctx, bool integer, bool phi, const PassArgs& A, double* gb,
-                            double* gg) {
-    if (phi) {
-        FQ_CHECK(schedule_for(A.tmask) == SC_L021, FQ_ERR_INVALID, "adjoint phase pass mask");
-        return integer ? launch_dual<int, true, SC_L021, GM>(ctx, A, gb, gg)
-                       : launch_dual<double, true, SC_L021, GM>(ctx, A, gb, gg);
-    }
-    switch (schedule_for(A.tmask)) {
-        case SC_L021: return launch_dual<int, false, SC_L021, GM>(ctx, A, gb, gg);
-        case SC_L01: return launch_dual<int, false, SC_L01, GM>(ctx, A, gb, gg);
-        default: return launch_dual<int, false, SC_L0, GM>(ctx, A, gb, gg);
-    }
-}
+// Destinations of the reverse sweep's partial sums: sum j (the grid
+// partials at part + j * grid) goes to out[dst[j]], or nowhere if -1.
+constexpr int kMaxGradSums = 768;
+struct GradSums {
+    int dst[kMaxGradSums];
+};
 
-static int dispatch_dual(fq_ctx* ctx, bool integer, bool phi, int gm, const PassArgs& A,
-                         double* gb, double* gg) {
-    return gm == GM_TAN ? dispatch_dual_gm<GM_TAN>(ctx, integer, phi, A, gb, gg)
-                        : dispatch_dual_gm<GM_COT>(ctx, integer, phi, A, gb, gg);
-}
-
-// One block per reverse pass q (in execution order: layers P-1..0, passes
-// 1..npass-1 then 0): the fixed-order sum of its grid dE/dbeta partials
-// (at part + q * stride) into out[1 + P + k * npass + i] and, for the
-// contiguous pass (i = 0), of its dE/dgamma partials (at + grid) into
-// out[1 + k].
-__global__ void k_reduce_grad(const double* part, int stride, int grid, int P, int npass,
-                              double* out) {
-    __shared__ double sh[2][256];
-    const int q = blockIdx.x;
-    const int k = P - 1 - q / npass, i = (q % npass + 1) % npass;
-    const double* pb = part + (size_t)q * stride;
-    double sb = 0, sg = 0;
-    for (int t = threadIdx.x; t < grid; t += 256) {
-        sb += pb[t];
-        if (i == 0) sg += pb[grid + t];
-    }
-    sh[0][threadIdx.x] = sb;
-    sh[1][threadIdx.x] = sg;
+// One block per sum, in a fixed order (deterministic results).
+__global__ void k_reduce_grad(const double* part, int grid, const GradSums S, double* out) {
+    __shared__ double sh[256];
+    const int j = blockIdx.x;
+    const int d = S.dst[j];
+    if (d < 0) return;  // uniform across the block
+    const double* pb = part + (size_t)j * grid;
+    double s = 0;
+    for (int t = threadIdx.x; t < grid; t += 256) s += pb[t];
+    sh[threadIdx.x] = s;
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
-            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
-        }
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        out[1 + P + k * npass + i] = sh[0][0];
-        if (i == 0) out[1 + k] = sh[1][0];
-    }
+    if (threadIdx.x == 0) out[d] = sh[0];
 }
 
 int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream) {
@@ -192,60 +157,100 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
         FQ_TRY(reduce_partials(ctx, ctx->d_partial, pass_grid(ctx, A, PH_NONE, false),
                                ctx->d_result));
     }
-    // Reverse sweep: per layer the strided passes, then the contiguous pass
-    // with dE/dgamma and the inverse phase.  RX(-beta) runs in reduced form
-    // f * G (gate_params): the kernels track the scale the vectors gain
-    // (1/f per rotation) and the contiguous pass multiplies f^N back in.
-    // Partials of every reverse pass go to their own segment of d_partial
-    // and are summed by one launch at the end (per-pass sums if they do not
-    // fit).  The two-level phase tables of the forward sweep are reused.
-    const int grid = (int)std::min<i64>(1ll << (N - kTileBits), (i64)ctx->num_sms);
-    const int seg = 2 * ctx->num_sms;
-    const bool batched = (i64)P * npass * seg <= ctx->partial_cap;
-    const bool all_tables = g.integer && engine_nhi(g) > 0 && P <= kMaxTableLayers;
-    int q = 0;
-    for (int k = P - 1; k >= 0; k--) {
-        int gm;
-        double gx, f;
-        gate_params(-betas[k], gm, gx, f);
-        int rotated = 0;  // qubits rotated so far in this layer's reverse sweep
-        const int nhi = g.integer ? engine_nhi(g) : 0;
-        if (g.integer && !all_tables) {
-            if (nhi > 0)
-                FQ_TRY(launch_table2(ctx, g, gammas[k]));
-            else
-                FQ_TRY(launch_table(ctx, g, gammas[k], 1.0));
+    // Reverse sweep.  Layer k visits its passes in the reverse of the
+    // forward order (descending plan order for even k, ascending for odd
+    // k); its last pass completes the layer's mixer, so it also takes
+    // dE/dgamma_k and the inverse phase, and shares its tile geometry with
+    // the first pass of layer k-1, which it runs too unless FQ_FUSE=0
+    // (sweeps: npass + (P-1)(npass-1) instead of P * npass).  RX(-beta)
+    // runs in reduced form f * G (gate_params): the kernels track the scale
+    // the vectors gain (1/f per rotation) and the phase pass multiplies f^N
+    // back in.  Each pass writes its partials (beta, gamma, the earlier
+    // layer's beta: grid each) to its own segment of d_partial, summed by
+    // one launch at the end (right after the pass if they do not fit).
+    // The two-level phase tables of the forward sweep are reused.
+    struct RevPass {
+        int k, i;    // layer, plan pass
+        bool phi;    // completes layer k's mixer
+        bool fused;  // also runs layer k-1's first pass
+    };
+    const bool fuse = fuse_enabled();
+    std::vector<RevPass> rev;
+    for (int k = P - 1; k >= 0; k--)
+        for (int j = 0; j < npass; j++) {
+            if (fuse && j == 0 && k < P - 1) continue;  // ran fused with layer k+1's last pass
+            const int i = (k % 2 == 0) ? npass - 1 - j : j;
+            const bool last = j == npass - 1;
+            rev.push_back({k, i, last, last && fuse && k > 0});
         }
-        for (int o = 1; o <= npass; o++, q++) {
-            const int i = o % npass;  // 1, 2, ..., npass-1, then 0
-            PassArgs A = base_args(ctx, sv, N, g);
-            A.sv2 = (double2*)costate;
-            A.l = plan[i].l;
-            A.a = plan[i].a;
-            A.tmask = plan[i].tmask;
-            A.gx = gx;
-            A.f2 = f * f;
-            A.sc0 = pow(f * f, rotated);
-            rotated += __builtin_popcount(plan[i].tmask);
+    const int nrev = (int)rev.size();
+    const int grid = (int)std::min<i64>(1ll << (N - kTileBits), (i64)ctx->num_sms);
+    const bool batched = (i64)nrev * 3 * grid <= ctx->partial_cap && 3 * nrev <= kMaxGradSums;
+    const bool all_tables = g.integer && engine_nhi(g) > 0 && P <= kMaxTableLayers;
+    const int nhi = g.integer ? engine_nhi(g) : 0;
+    std::vector<int> gm(P);
+    std::vector<double> gx(P), f(P);
+    for (int k = 0; k < P; k++) gate_params(-betas[k], gm[k], gx[k], f[k]);
+    std::vector<int> rotated(P, 0);  // qubits of layer k rotated so far
+    GradSums sums;
+    for (int j = 0; j < kMaxGradSums; j++) sums.dst[j] = -1;
+    for (int q = 0; q < nrev; q++) {
+        const RevPass& R = rev[q];
+        const int k = R.k, i = R.i;
+        PassArgs A = base_args(ctx, sv, N, g);
+        A.sv2 = (double2*)costate;
+        A.l = plan[i].l;
+        A.a = plan[i].a;
+        A.tmask = plan[i].tmask;
+        const int nt = __builtin_popcount(plan[i].tmask);
+        A.gx = gx[k];
+        A.f2 = f[k] * f[k];
+        A.sc0 = pow(f[k] * f[k], rotated[k]);
+        rotated[k] += nt;
+        double* gb = ctx->d_partial + (batched ? (size_t)q * 3 * grid : 0);
+        double* gg = gb + grid;
+        double* gb2 = gb + 2 * grid;
+        const int dst_b = 1 + P + k * npass + i, dst_g = 1 + k;
+        const int dst_b2 = 1 + P + (k - 1) * npass + i;
+        if (!R.phi) {
+            FQ_TRY(dispatch_dual_rx(ctx, gm[k], A, gb));
+        } else {
+            if (g.integer && !all_tables) {
+                if (nhi > 0)
+                    FQ_TRY(launch_table2(ctx, g, gammas[k]));
+                else
+                    FQ_TRY(launch_table(ctx, g, gammas[k], 1.0));
+            }
             A.gamma = gammas[k];
             if (nhi > 0) set_table_args(A, g, gammas[k], 1.0);
             if (all_tables) A.ptab = ctx->d_ptab + (size_t)k * kTableStride;
             A.tree = phase_tree_ok(g, gammas[k]) ? 1 : 0;
             // Inverse phase (times f^N) only where layers remain.
-            A.scale = k > 0 ? pow(f, N) : 0.0;
-            double* gb = ctx->d_partial + (batched ? (size_t)q * seg : 0);
-            double* gg = gb + grid;
-            FQ_TRY(dispatch_dual(ctx, g.integer, i == 0, gm, A, gb, gg));
-            if (!batched) {
-                FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + 1 + P + k * npass + i));
-                if (i == 0) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + 1 + k));
+            A.scale = k > 0 ? pow(f[k], N) : 0.0;
+            int gm2 = GM_NONE;
+            if (R.fused) {
+                gm2 = gm[k - 1];
+                A.gx2 = gx[k - 1];
+                A.f2b = f[k - 1] * f[k - 1];
+                rotated[k - 1] += nt;
             }
+            FQ_TRY(g.integer ? dispatch_dual_phase_int(ctx, gm[k], gm2, A, gb, gg, gb2)
+                             : dispatch_dual_phase_fp(ctx, gm[k], gm2, A, gb, gg, gb2));
+        }
+        if (batched) {
+            sums.dst[3 * q] = dst_b;
+            if (R.phi) sums.dst[3 * q + 1] = dst_g;
+            if (R.fused) sums.dst[3 * q + 2] = dst_b2;
+        } else {
+            FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + dst_b));
+            if (R.phi) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + dst_g));
+            if (R.fused) FQ_TRY(reduce_partials(ctx, gb2, grid, ctx->d_result + dst_b2));
         }
     }
     if (batched) {
         const int tok = prof_begin(ctx);
-        k_reduce_grad<<<P * npass, 256, 0, ctx->stream>>>(ctx->d_partial, seg, grid, P, npass,
-                                                          ctx->d_result);
+        k_reduce_grad<<<3 * nrev, 256, 0, ctx->stream>>>(ctx->d_partial, grid, sums,
+                                                         ctx->d_result);
         FQ_CUDA(cudaGetLastError());
         prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
         ctx->launches++;

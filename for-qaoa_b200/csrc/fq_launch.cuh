@@ -240,6 +240,14 @@ int dispatch_fused_fp(fq_ctx* ctx, int gm1, int gm2, const PassArgs& A);
 inline int dispatch_fused(fq_ctx* ctx, bool integer, int gm1, int gm2, const PassArgs& A) {
     return integer ? dispatch_fused_int(ctx, gm1, gm2, A) : dispatch_fused_fp(ctx, gm1, gm2, A);
 }
+// Adjoint pass that completes a layer's mixer (k_pass_dual with PHI):
+// RX(-beta) (gm, A.gx) on A.tmask, dE/dgamma and the inverse phase, then
+// with gm2 != GM_NONE the earlier layer's RX(-beta) (gm2, A.gx2) on A.tmask.
+// Partials: gb (beta), gg (gamma), gb2 (the earlier layer's beta).
+int dispatch_dual_phase_int(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
+                            double* gg, double* gb2);
+int dispatch_dual_phase_fp(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
+                           double* gg, double* gb2);
 // Read-only sweeps: <C> partials or the cut diagonal (diag != 0).
 int dispatch_readonly(fq_ctx* ctx, bool integer, bool diag, const PassArgs& A);
 // <C> partials and the costate A.sv2 = C * A.sv.

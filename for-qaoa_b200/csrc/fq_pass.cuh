@@ -96,6 +96,7 @@ struct PassArgs {
     int tree;        // FP64 weights: phases by product tree (else one sincos per amplitude)
     double sc0, f2;  // adjoint passes: scale of the inner products at the pass's start, and
                      // the factor (f^2) it gains with every reduced rotation
+    double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
     int* err;        // device error flag (bounded waits that gave up)
 };

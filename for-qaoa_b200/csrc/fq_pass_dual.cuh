@@ -108,34 +108,44 @@ __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[
 // while the kernel sets up), then the tables of k_pass.
 template <typename WT>
 __host__ __device__ inline size_t dual_smem_bytes(int) {
-    return 2 * sizeof(double2) * kTile + PassSmem<WT>::bytes + 16 * sizeof(double);
+    return 2 * sizeof(double2) * kTile + PassSmem<WT>::bytes + 24 * sizeof(double);
 }
 
 // RX(-beta) in reduced form GM (A.gx = t or u, A.f2 = f^2, A.sc0 = scale of
-// the vectors at the pass's start, see rx_regs_dual).  PHI: this pass also
-// accumulates dE/dgamma (-Im<w|S|v>, negated on the host) and, if
-// A.scale != 0, multiplies both vectors by the conjugate phase times A.scale
-// = f^N, which returns them to their true scale for the next layer.  ST:
-// write the vectors back.  Partials: gb[blockIdx] (beta) and
-// gg[blockIdx] (gamma).  The next tile of both vectors is prefetched into
-// L2 while the current one is computed (one CTA per SM cannot hide the
-// HBM latency of its loads otherwise).
-template <typename WT, bool PHI, int SC, bool ST, int GM>
+// the vectors at the pass's start, see rx_regs_dual) on the pass's targets,
+// dE/dbeta partials to gb.  PHI: the pass completes its layer's mixer, so it
+// also accumulates dE/dgamma (-Im<w|S|v>, negated on the host) into gg and,
+// if A.scale != 0, multiplies both vectors by the conjugate phase times
+// A.scale = f^N, which returns them to their true scale.  GM2 != GM_NONE (a
+// fused pass, PHI only): then RX(-beta) of the layer before (GM2, A.gx2,
+// A.f2b) on the same targets, from scale 1, its dE/dbeta partials to gb2.
+// With the reverse pass order alternating from layer to layer, the last
+// pass of one layer and the first of the next share a tile geometry, so two
+// sweeps become one.  The phase and dE/dgamma are taken in the layout the
+// first rounds end in (L1, or L0 with SC_L0).  ST: write the vectors back.
+// The next tile of both vectors is prefetched into L2 while the current one
+// is computed (one CTA per SM cannot hide the HBM latency of its loads
+// otherwise).
+template <typename WT, bool PHI, int SC, bool ST, int GM, int GM2 = GM_NONE>
 __global__ void __launch_bounds__(kPassThreads, 1)
-    k_pass_dual(const PassArgs A, double* gb, double* gg) {
+    k_pass_dual(const PassArgs A, double* gb, double* gg, double* gb2) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
     double2* buf = reinterpret_cast<double2*>(smraw);
     unsigned char* const sm = smraw + 2 * sizeof(double2) * kTile;
     const CutTables<WT> ct(sm);
     double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
-    double* red = reinterpret_cast<double*>(sm + SM::bytes);  // 16: beta and gamma partials
+    double* red = reinterpret_cast<double*>(sm + SM::bytes);  // 24: the three partials
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
     const int nmid = a - l;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr bool CUT = PHI;
     constexpr bool INTW = sizeof(WT) == sizeof(int);
+    constexpr bool FUSED = GM2 != GM_NONE;
+    static_assert(PHI || !FUSED, "a fused adjoint pass carries its layer's phase");
+    constexpr int LP = SC == SC_L0 ? 0 : 1;  // layout after the first rounds
+    constexpr int LAY = FUSED ? 0 : LP;       // layout of the stores
 
     WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
     if (CUT) {
@@ -166,7 +176,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const int pf_step = l < 3 ? l : 3;
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
-    double accb = 0, accg = 0;
+    double accb = 0, accg = 0, accb2 = 0;
     const double g = A.gx, f2 = A.f2;
 
     int par = 0;
@@ -198,12 +208,13 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         }
         WT* const kp = ct.ke + 32 * par;
         if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // read after the exchanges' barriers
+        // First rounds: L0 -> (L2 ->) L1, or L0 only with SC_L0.  The
+        // previous tile's readers of buf are done once every thread is past
+        // this tile's first barrier (the leading barrier of its first
+        // exchange, a block barrier).
         double sc = A.sc0;
         rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
         if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
-        // The previous tile's readers of buf are done once every thread is
-        // past this tile's first barrier: with the cut barrier (CUT) or the
-        // leading barrier of the first exchange.
         if (SC == SC_L021) {
             exchange_dual<0, 2>(v, w, buf, tid, true);
             rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
@@ -211,21 +222,18 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         } else if (SC == SC_L01) {
             exchange_dual<0, 1>(v, w, buf, tid, true);
         }
-        constexpr int LAY = (SC != SC_L0 && !PHI) ? 1 : 0;
-        if (SC != SC_L0) {
-            rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
-            if (LAY == 0) exchange_dual<1, 0>(v, w, buf, tid, true);
-        }
-        if (PHI) {
+        if (SC != SC_L0) rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
+        if constexpr (PHI) {
             if (SC == SC_L0) __syncthreads();  // kp written by warps 0 and 1
             WT cbase, g0, g1, g2, g3;
-            ct.consts(kp, tid, cbase, g0, g1, g2, g3);
+            ct.template consts<LP>(kp, tid, cbase, g0, g1, g2, g3);
+            const WT* crg = ct.creg + 16 * LP;
+            const double2* qt = ct.qtab + 16 * LP;
             double tg = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
-                              ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
-                              ((r & 8) ? g3 : WT(0));
+                const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 const double S = 2.0 * (double)cr - A.W;
                 tg = fma(w[r].x * v[r].y - w[r].y * v[r].x, S, tg);
             }
@@ -244,7 +252,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                     const double2 H[4] = {make_double2(1.0, 0.0), E2, E3, cmul(E2, E3)};
 #pragma unroll
                     for (int r = 0; r < kRegs; r++) {
-                        double2 ph = cmul(L[r & 3], ct.qtab[r]);
+                        double2 ph = cmul(L[r & 3], qt[r]);
                         if (r >> 2) ph = cmul(ph, H[r >> 2]);
                         const double2 c = make_double2(ph.x, -ph.y);
                         v[r] = cmul(v[r], c);
@@ -253,7 +261,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 } else {  // one phase per amplitude: global table or sincos
 #pragma unroll
                     for (int r = 0; r < kRegs; r++) {
-                        const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
+                        const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) +
                                       ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
                                       ((r & 8) ? g3 : WT(0));
                         double2 ph;
@@ -269,6 +277,23 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                         w[r] = cmul(w[r], c);
                     }
                 }
+            }
+            if constexpr (FUSED) {
+                // The earlier layer's rounds in the opposite order, back to
+                // L0 (a single target among tile bits 0..3 is the same lane
+                // bit in L1 as in L0).
+                double sc2 = 1.0;
+                const double g2x = A.gx2, f2b = A.f2b;
+                if (SC != SC_L0) rx_regs_dual<GM2>(v, w, m_mid, g2x, f2b, sc2, accb2);
+                if (lo_lane >= 0) rx_lane_dual<GM2>(v, w, lo_lane, g2x, f2b, sc2, accb2);
+                if (SC == SC_L021) {
+                    exchange_dual<1, 2>(v, w, buf, tid, true);
+                    rx_regs_dual<GM2>(v, w, m_lo, g2x, f2b, sc2, accb2);
+                    exchange_dual<2, 0>(v, w, buf, tid, true);
+                } else if (SC == SC_L01) {
+                    exchange_dual<1, 0>(v, w, buf, tid, true);
+                }
+                rx_regs_dual<GM2>(v, w, m_hi, g2x, f2b, sc2, accb2);
             }
         }
         if (ST) {
@@ -293,21 +318,25 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     for (int o = 16; o > 0; o >>= 1) {
         accb += __shfl_xor_sync(0xffffffffu, accb, o);
         accg += __shfl_xor_sync(0xffffffffu, accg, o);
+        accb2 += __shfl_xor_sync(0xffffffffu, accb2, o);
     }
     __syncthreads();
     if (lane == 0) {
         red[warp] = accb;
         red[8 + warp] = accg;
+        red[16 + warp] = accb2;
     }
     __syncthreads();
     if (tid == 0) {
-        double sb = 0, sg = 0;
+        double sb = 0, sg = 0, sb2 = 0;
         for (int k = 0; k < kPassThreads / 32; k++) {
             sb += red[k];
             sg += red[8 + k];
+            sb2 += red[16 + k];
         }
         gb[blockIdx.x] = sb;
         if (PHI) gg[blockIdx.x] = sg;
+        if (FUSED) gb2[blockIdx.x] = sb2;
     }
 }
 

@@ -1,11 +1,18 @@
 """GPU tests of the adjoint gradient (fq_qaoa_energy_grad): against the FP64
 CPU adjoint of the oracle (1e-8, relative to max(1, |g|)), against central
-finite differences of the GPU energy, and the benchmark config of 26 qubits
-and 10 layers."""
+finite differences of the GPU energy, the benchmark config of 26 qubits and
+10 layers, and the reverse sweep's two schedules (fused two-layer passes,
+the default, and one sweep per pass with FQ_FUSE=0) over every tile
+schedule a layer-completing pass can have."""
+import json
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
-from conftest import ENERGY_RTOL, GRAD_TOL, complete_int, gnp_fp, gnp_int, angles
+from conftest import ENERGY_RTOL, GRAD_TOL, PKG, complete_int, gnp_fp, gnp_int, angles
 
 pytestmark = pytest.mark.gpu
 
@@ -86,3 +93,48 @@ def test_energy_grad_matches_forward_energy(ctx):
     finally:
         st.free()
     assert abs(e - ef) <= ENERGY_RTOL * abs(ef)
+
+
+GRAD_CHILD = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, %(pkg)r)
+import forqaoa
+cases = json.loads(sys.stdin.read())
+out = []
+with forqaoa.Context(0) as ctx:
+    for c in cases:
+        e, gg, gb = ctx.energy_grad(c["n"], np.array(c["W"]), np.array(c["g"]), np.array(c["b"]))
+        out.append({"e": e, "gg": gg.tolist(), "gb": gb.tolist()})
+print(json.dumps(out))
+"""
+
+
+# The pass that completes a layer alternates between the contiguous pass and
+# the last strided pass, whose tile schedule is L0 (N 13..16, 24), L01
+# (17..21, 25..30) or L021 (22, 23); P = 1 has no fused pass; "huge" weights
+# take one phase table per layer, FP64 weights with a large sum ("wide" plus
+# a quarter) one sincos per amplitude.
+@pytest.mark.parametrize("fuse", ["1", "0"])
+def test_reverse_schedules_match_oracle(oracle, fuse):
+    rng = np.random.default_rng(404)
+    cs = []
+    for n, P, kind in ((13, 3, "int"), (16, 4, "fp"), (17, 2, "neg"), (20, 5, "int"),
+                       (22, 3, "int"), (23, 4, "fp"), (24, 3, "int"), (24, 2, "huge"),
+                       (21, 5, "wide"), (19, 4, "huge"), (25, 1, "int"), (18, 6, "sparse")):
+        W = graph_of(kind, n, rng)
+        if kind == "wide":
+            W = W + 0.25 * (W > 0)
+        g, b = angles(rng, P)
+        cs.append({"n": n, "W": W.tolist(), "g": g.tolist(), "b": b.tolist()})
+    env = dict(os.environ, FQ_FUSE=fuse)
+    res = subprocess.run([sys.executable, "-c", GRAD_CHILD % {"pkg": PKG}],
+                         input=json.dumps(cs), capture_output=True, text=True, env=env,
+                         timeout=900)
+    assert res.returncode == 0, res.stderr[-2000:]
+    got = json.loads(res.stdout.strip().splitlines()[-1])
+    for c, r in zip(cs, got):
+        eo, ggo, gbo = oracle.energy_grad(np.array(c["W"]), np.array(c["g"]), np.array(c["b"]))
+        assert abs(r["e"] - eo) <= ENERGY_RTOL * abs(eo), c["n"]
+        check_grad(r["gg"], ggo)
+        check_grad(r["gb"], gbo)
