@@ -38,17 +38,20 @@ __device__ __forceinline__ void rx_regs_dual(double2 (&v)[kRegs], double2 (&w)[k
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         if ((m4 >> k) & 1u) {
-            double t = 0;
+            double ta = 0, tb = 0;  // two FMA chains
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 if (!((r >> k) & 1)) {
                     const int q = r | (1 << k);
-                    t += (w[r].x * v[q].y - w[r].y * v[q].x) + (w[q].x * v[r].y - w[q].y * v[r].x);
+                    ta = fma(w[r].x, v[q].y, ta);
+                    ta = fma(-w[r].y, v[q].x, ta);
+                    tb = fma(w[q].x, v[r].y, tb);
+                    tb = fma(-w[q].y, v[r].x, tb);
                     rx_pair<GM>(v[r], v[q], g, 0.0, 0.0);
                     rx_pair<GM>(w[r], w[q], g, 0.0, 0.0);
                 }
             }
-            acc = fma(sc, t, acc);
+            acc = fma(sc, ta + tb, acc);
             sc *= f2;
         }
     }
@@ -67,7 +70,8 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
         pv.y = __shfl_xor_sync(0xffffffffu, v[r].y, lm);
         pw.x = __shfl_xor_sync(0xffffffffu, w[r].x, lm);
         pw.y = __shfl_xor_sync(0xffffffffu, w[r].y, lm);
-        t += w[r].x * pv.y - w[r].y * pv.x;
+        t = fma(w[r].x, pv.y, t);
+        t = fma(-w[r].y, pv.x, t);
         const double2 mv = v[r], mw = w[r];
         if (GM == GM_TAN) {
             v[r].x = fma(g, pv.y, mv.x);
@@ -83,6 +87,15 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
     }
     acc = fma(sc, t, acc);
     sc *= f2;
+}
+
+// x through an empty volatile asm inside the tile loop: the compiler must
+// take it as a new value there, so what is derived from it (addresses) is
+// recomputed where it is used instead of being hoisted out of the loop and
+// held in registers the 32 amplitudes of a thread need.
+__device__ __forceinline__ i64 opaque(i64 x) {
+    asm volatile("" : "+l"(x));
+    return x;
 }
 
 template <int LF, int LT>
@@ -163,11 +176,9 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const i64 s10 = 1ll << tile_phys(10, l, a), s11 = 1ll << tile_phys(11, l, a);
     const i64 s4 = 1ll << tile_phys(4, l, a), s5 = 1ll << tile_phys(5, l, a);
     const i64 s6 = 1ll << tile_phys(6, l, a), s7 = 1ll << tile_phys(7, l, a);
-    auto off0 = [&](int r) -> i64 {
-        return ((r & 1) ? s8 : 0) + ((r & 2) ? s9 : 0) + ((r & 4) ? s10 : 0) + ((r & 8) ? s11 : 0);
-    };
-    auto off1 = [&](int r) -> i64 {
-        return ((r & 1) ? s4 : 0) + ((r & 2) ? s5 : 0) + ((r & 4) ? s6 : 0) + ((r & 8) ? s7 : 0);
+    // Offset of register slot r from strides (b0..b3) of its 4 bits.
+    auto offr = [](int r, i64 b0, i64 b1, i64 b2, i64 b3) -> i64 {
+        return ((r & 1) ? b0 : 0) + ((r & 2) ? b1 : 0) + ((r & 4) ? b2 : 0) + ((r & 8) ? b3 : 0);
     };
     auto tile_base = [&](i64 T) -> i64 {
         return ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
@@ -182,13 +193,15 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     int par = 0;
     for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
         const i64 base = tile_base(T);
-        double2* const pv = A.sv + base + thr_off;
-        double2* const pw = A.sv2 + base + thr_off;
         double2 v[kRegs], w[kRegs];
+        {
+            const i64 o = opaque(base + thr_off);
+            const i64 b8 = opaque(s8), b9 = opaque(s9), b10 = opaque(s10), b11 = opaque(s11);
 #pragma unroll
-        for (int r = 0; r < kRegs; r++) {
-            v[r] = __ldcs(pv + off0(r));
-            w[r] = __ldcs(pw + off0(r));
+            for (int r = 0; r < kRegs; r++) {
+                v[r] = __ldcs(A.sv + o + offr(r, b8, b9, b10, b11));
+                w[r] = __ldcs(A.sv2 + o + offr(r, b8, b9, b10, b11));
+            }
         }
         if (T + gridDim.x < A.ntiles) {
             const i64 b2 = tile_base(T + gridDim.x);
@@ -208,6 +221,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         }
         WT* const kp = ct.ke + 32 * par;
         if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // read after the exchanges' barriers
+        // The thread index re-read in every tile: the exchange addresses
+        // derived from it are recomputed (a few integer ops) instead of being
+        // hoisted out of the loop, where they would take registers.
+        int xt;
+        asm volatile("mov.u32 %0, %%tid.x;" : "=r"(xt));
         // First rounds: L0 -> (L2 ->) L1, or L0 only with SC_L0.  The
         // previous tile's readers of buf are done once every thread is past
         // this tile's first barrier (the leading barrier of its first
@@ -216,11 +234,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
         if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
         if (SC == SC_L021) {
-            exchange_dual<0, 2>(v, w, buf, tid, true);
+            exchange_dual<0, 2>(v, w, buf, xt, true);
             rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
-            exchange_dual<2, 1>(v, w, buf, tid, true);
+            exchange_dual<2, 1>(v, w, buf, xt, true);
         } else if (SC == SC_L01) {
-            exchange_dual<0, 1>(v, w, buf, tid, true);
+            exchange_dual<0, 1>(v, w, buf, xt, true);
         }
         if (SC != SC_L0) rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
         if constexpr (PHI) {
@@ -242,21 +260,31 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 if (INTW ? A.nhi > 0 : A.tree != 0) {  // product tree (see k_pass)
                     double2 P = phase_of<WT>(A, smtab, cbase);
                     if (INTW) P = make_double2(P.x * A.scale, P.y * A.scale);
-                    // Registers are plentiful here (one CTA per SM): build
-                    // every slot's phase once from L = P * {1, E0, E1, E0 E1}
-                    // and H = {1, E2, E3, E2 E3} and apply its conjugate to
-                    // both vectors.
-                    const double2 E0 = zpow<WT>(A, smtab, g0), E1 = zpow<WT>(A, smtab, g1);
-                    const double2 E2 = zpow<WT>(A, smtab, g2), E3 = zpow<WT>(A, smtab, g3);
-                    const double2 L[4] = {P, cmul(P, E0), cmul(P, E1), cmul(cmul(P, E0), E1)};
-                    const double2 H[4] = {make_double2(1.0, 0.0), E2, E3, cmul(E2, E3)};
+                    // Two stages, to keep few values live next to the 32
+                    // amplitudes: the conjugate of L[r & 3] * Q_r with
+                    // L = P * {1, E0, E1, E0 E1} on every slot, then that of
+                    // H[r >> 2], H = {1, E2, E3, E2 E3}.
+                    {
+                        const double2 E0 = zpow<WT>(A, smtab, g0), E1 = zpow<WT>(A, smtab, g1);
+                        const double2 L[4] = {P, cmul(P, E0), cmul(P, E1),
+                                              cmul(cmul(P, E0), E1)};
 #pragma unroll
-                    for (int r = 0; r < kRegs; r++) {
-                        double2 ph = cmul(L[r & 3], qt[r]);
-                        if (r >> 2) ph = cmul(ph, H[r >> 2]);
-                        const double2 c = make_double2(ph.x, -ph.y);
-                        v[r] = cmul(v[r], c);
-                        w[r] = cmul(w[r], c);
+                        for (int r = 0; r < kRegs; r++) {
+                            const double2 ph = cmul(L[r & 3], qt[r]);
+                            const double2 c = make_double2(ph.x, -ph.y);
+                            v[r] = cmul(v[r], c);
+                            w[r] = cmul(w[r], c);
+                        }
+                    }
+                    {
+                        const double2 E2 = zpow<WT>(A, smtab, g2), E3 = zpow<WT>(A, smtab, g3);
+                        const double2 H[4] = {make_double2(1.0, 0.0), E2, E3, cmul(E2, E3)};
+#pragma unroll
+                        for (int r = 4; r < kRegs; r++) {
+                            const double2 c = make_double2(H[r >> 2].x, -H[r >> 2].y);
+                            v[r] = cmul(v[r], c);
+                            w[r] = cmul(w[r], c);
+                        }
                     }
                 } else {  // one phase per amplitude: global table or sincos
 #pragma unroll
@@ -287,29 +315,31 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 if (SC != SC_L0) rx_regs_dual<GM2>(v, w, m_mid, g2x, f2b, sc2, accb2);
                 if (lo_lane >= 0) rx_lane_dual<GM2>(v, w, lo_lane, g2x, f2b, sc2, accb2);
                 if (SC == SC_L021) {
-                    exchange_dual<1, 2>(v, w, buf, tid, true);
+                    exchange_dual<1, 2>(v, w, buf, xt, true);
                     rx_regs_dual<GM2>(v, w, m_lo, g2x, f2b, sc2, accb2);
-                    exchange_dual<2, 0>(v, w, buf, tid, true);
+                    exchange_dual<2, 0>(v, w, buf, xt, true);
                 } else if (SC == SC_L01) {
-                    exchange_dual<1, 0>(v, w, buf, tid, true);
+                    exchange_dual<1, 0>(v, w, buf, xt, true);
                 }
                 rx_regs_dual<GM2>(v, w, m_hi, g2x, f2b, sc2, accb2);
             }
         }
         if (ST) {
             if (LAY == 0) {
+                const i64 o = opaque(base + thr_off);
+                const i64 b8 = opaque(s8), b9 = opaque(s9), b10 = opaque(s10), b11 = opaque(s11);
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    __stcs(pv + off0(r), v[r]);
-                    __stcs(pw + off0(r), w[r]);
+                    __stcs(A.sv + o + offr(r, b8, b9, b10, b11), v[r]);
+                    __stcs(A.sv2 + o + offr(r, b8, b9, b10, b11), w[r]);
                 }
             } else {
-                double2* const qv = A.sv + base + thr_off1;
-                double2* const qw = A.sv2 + base + thr_off1;
+                const i64 o = opaque(base + thr_off1);
+                const i64 b4 = opaque(s4), b5 = opaque(s5), b6 = opaque(s6), b7 = opaque(s7);
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
-                    __stcs(qv + off1(r), v[r]);
-                    __stcs(qw + off1(r), w[r]);
+                    __stcs(A.sv + o + offr(r, b4, b5, b6, b7), v[r]);
+                    __stcs(A.sv2 + o + offr(r, b4, b5, b6, b7), w[r]);
                 }
             }
         }
