@@ -2,8 +2,10 @@
 load pass (FQ_TMA=0), the default mix (1), the two-group TMA pass (2) and
 the one-group TMA pass for every read-write sweep (3), with and without the
 L2 prefetch, the strided passes as the warp-specialised pipeline with TMA
-stores (FQ_WS=1) or the one-group TMA pass (FQ_WS=0, the default), and the
-fused two-layer schedule (FQ_FUSE=1, the default) or one sweep per pass.
+stores (FQ_WS=1) or the one-group TMA pass (FQ_WS=0, the default), the
+fused two-layer schedule (FQ_FUSE=1, the default) or one sweep per pass,
+and the fused passes as TMA pipelines (FQ_TMAF=2 all, 1 the strided ones,
+0 none, the default).
 The mode is read once per process, so each runs in a child process; states and <C> are checked against the oracle."""
 import json
 import os
@@ -40,7 +42,7 @@ def cases():
     rng = np.random.default_rng(77)
     out = []
     for n, kind, P in ((13, "int", 2), (16, "fp", 3), (18, "int", 2), (20, "int", 3),
-                       (21, "fp", 1), (17, "neg", 2)):
+                       (21, "fp", 1), (17, "neg", 2), (21, "int", 4), (19, "fp", 3)):
         W = {"int": complete_int(n, rng), "fp": gnp_fp(n, rng),
              "neg": complete_int(n, rng, -6, 6)}[kind]
         g, b = angles(rng, P)
@@ -48,13 +50,15 @@ def cases():
     return out
 
 
-@pytest.mark.parametrize("tma,prefetch,ws,fuse", [
-    ("0", "0", "1", "1"), ("1", "1", "1", "1"), ("1", "1", "0", "1"), ("2", "0", "1", "1"),
-    ("3", "1", "1", "1"), ("1", "1", "0", "0"), ("0", "0", "0", "0"),
+@pytest.mark.parametrize("tma,prefetch,ws,fuse,tmaf", [
+    ("0", "0", "1", "1", "1"), ("1", "1", "1", "1", "1"), ("1", "1", "0", "1", "1"),
+    ("2", "0", "1", "1", "0"), ("3", "1", "1", "1", "0"), ("1", "1", "0", "0", "0"),
+    ("0", "0", "0", "0", "0"), ("1", "1", "0", "1", "0"), ("1", "1", "0", "1", "2"),
 ])
-def test_pass_modes_match_oracle(oracle, tma, prefetch, ws, fuse):
+def test_pass_modes_match_oracle(oracle, tma, prefetch, ws, fuse, tmaf):
     cs = cases()
-    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws, FQ_FUSE=fuse)
+    env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws, FQ_FUSE=fuse,
+               FQ_TMAF=tmaf)
     res = subprocess.run([sys.executable, "-c", CHILD % {"pkg": PKG}], input=json.dumps(cs),
                          capture_output=True, text=True, env=env, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
