@@ -98,10 +98,21 @@ struct PassArgs {
                      // the factor (f^2) it gains with every reduced rotation
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
+    int trot;        // tile order: rotation of the fixed bits below the high tile bits (tile_mid)
     int* err;        // device error flag (bounded waits that gave up)
 };
 
 __device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j : a + j - l; }
+
+// The nmid fixed bits of tile number T that lie between the row bits and the
+// high tile bits, rotated left by rot (none unless 0 < rot < nmid): tiles
+// with consecutive numbers -- the ones the CTAs of a grid work on at the
+// same moment -- then differ in higher address bits.  A bijection on the
+// tiles of a pass, so any rotation visits each tile once.
+__device__ __forceinline__ i64 tile_mid(i64 T, int nmid, int rot) {
+    const i64 mask = (1ll << nmid) - 1, m = T & mask;
+    return (rot > 0 && rot < nmid) ? (((m << rot) | (m >> (nmid - rot))) & mask) : m;
+}
 
 constexpr int kPhaseLo = 32;     // low-part entries of the two-level phase table
 constexpr int kPhaseHiMax = 512; // high-part entries kept in shared memory at most
@@ -201,6 +212,20 @@ __device__ __forceinline__ void rx_lane(double2 (&v)[kRegs], int j, double g, do
             v[r].y = m.y * c - q.x * s;
         }
     }
+}
+
+// x through an empty volatile asm inside a tile loop: the compiler must take
+// it as a new value there, so what is derived from it (addresses) is
+// recomputed where it is used instead of being hoisted out of the loop and
+// held in registers the amplitudes of a thread need (the adjoint pass).
+__device__ __forceinline__ i64 opaque(i64 x) {
+    asm volatile("" : "+l"(x));
+    return x;
+}
+
+// Offset of register slot r from the strides b0..b3 of its 4 tile bits.
+__device__ __forceinline__ i64 offr(int r, i64 b0, i64 b1, i64 b2, i64 b3) {
+    return ((r & 1) ? b0 : 0) + ((r & 2) ? b1 : 0) + ((r & 4) ? b2 : 0) + ((r & 8) ? b3 : 0);
 }
 
 // Tile index held in register r under layout L (see header comment).

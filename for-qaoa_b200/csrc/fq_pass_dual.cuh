@@ -89,15 +89,6 @@ __device__ __forceinline__ void rx_lane_dual(double2 (&v)[kRegs], double2 (&w)[k
     sc *= f2;
 }
 
-// x through an empty volatile asm inside the tile loop: the compiler must
-// take it as a new value there, so what is derived from it (addresses) is
-// recomputed where it is used instead of being hoisted out of the loop and
-// held in registers the 32 amplitudes of a thread need.
-__device__ __forceinline__ i64 opaque(i64 x) {
-    asm volatile("" : "+l"(x));
-    return x;
-}
-
 template <int LF, int LT>
 __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[kRegs],
                                               double2* buf, int tid, bool wait_readers = true) {
@@ -176,10 +167,6 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const i64 s10 = 1ll << tile_phys(10, l, a), s11 = 1ll << tile_phys(11, l, a);
     const i64 s4 = 1ll << tile_phys(4, l, a), s5 = 1ll << tile_phys(5, l, a);
     const i64 s6 = 1ll << tile_phys(6, l, a), s7 = 1ll << tile_phys(7, l, a);
-    // Offset of register slot r from strides (b0..b3) of its 4 bits.
-    auto offr = [](int r, i64 b0, i64 b1, i64 b2, i64 b3) -> i64 {
-        return ((r & 1) ? b0 : 0) + ((r & 2) ? b1 : 0) + ((r & 4) ? b2 : 0) + ((r & 8) ? b3 : 0);
-    };
     auto tile_base = [&](i64 T) -> i64 {
         return ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
     };

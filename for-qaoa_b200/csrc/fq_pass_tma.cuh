@@ -100,7 +100,7 @@ __device__ __forceinline__ int tslot(int t) { return t ^ ((t >> 3) & 7); }
 template <typename WT>
 __host__ __device__ inline size_t tma_pass_smem_bytes(int N) {
     return 1024 + (size_t)kStages * kTileBytes + 64 + sizeof(double) * 8 + sizeof(i64) * 32 +
-           sizeof(int) * 24 + sizeof(WT) * (N * N + 32 + 16 + 24 + 16) + 16 +
+           sizeof(int) * 24 + sizeof(WT) * (N * N + 32 + 16 + 24 + 16 + 16) + 16 +
            (sizeof(WT) == sizeof(int) ? phase_smem_bytes() : 0);
 }
 
@@ -121,9 +121,13 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     WT* creg = ke + 32;
     WT* Dm = creg + 16;
     WT* Ru = Dm + 24;
+    WT* creg1 = Ru + 16;  // register-bit cut table of layout L1 (E1)
     double2* smtab = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);
+        (reinterpret_cast<uintptr_t>(creg1 + 16) + 15) & ~(uintptr_t)15);
     constexpr bool CUT = (PH != PH_NONE) || (EX == EX_ENERGY);
+    // <C> of a pass whose rounds end in layout L1 is taken there (constants
+    // of L1), so the tile leaves from L1 without a change back to L0.
+    constexpr bool E1 = EX == EX_ENERGY && GM != GM_NONE && SC != SC_L0;
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
     const int nmid = a - l;
@@ -140,10 +144,10 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         if (G.kind == TG_CONTIG) {
             tma_load_3d(dst, &tmap, &full[s], 0, 0, (int)(2 * T));
         } else if (G.kind == TG_ROWS) {
-            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)(T & ((1ll << nmid) - 1)), 0,
+            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)tile_mid(T, nmid, A.trot), 0,
                         (int)(T >> nmid));
         } else {
-            tma_load_5d(dst, &tmap, &full[s], 0, (int)(T & ((1ll << nmid) - 1)), 0, 0,
+            tma_load_5d(dst, &tmap, &full[s], 0, (int)tile_mid(T, nmid, A.trot), 0, 0,
                         (int)(T >> nmid));
         }
     };
@@ -188,6 +192,14 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                     if (((r >> k) ^ (r >> k2)) & 1)
                         c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
             creg[r] = c;
+        } else if (E1 && tid >= 96 && tid < 112) {
+            const int r = tid - 96;
+            WT c = 0;
+            for (int k = 0; k < 4; k++)
+                for (int k2 = k + 1; k2 < 4; k2++)
+                    if (((r >> k) ^ (r >> k2)) & 1)
+                        c += sw[tile_phys(4 + k, l, a) * N + tile_phys(4 + k2, l, a)];
+            creg1[r] = c;
         }
     }
     WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
@@ -213,13 +225,39 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             }
         }
     }
+    // The same per-thread constants for layout L1: thread bits 0..3 and
+    // 8..11 of slot 0's tile index, register bits 4..7.
+    const int t1 = lay_index<1>(tid, 0);
+    WT athr1 = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    if (E1) {
+        for (int jj = 0; jj < 8; jj++) {
+            const int bj = jj < 4 ? jj : jj + 4;
+            const int pj = tile_phys(bj, l, a);
+            const int tj = (t1 >> bj) & 1;
+            for (int j2 = jj + 1; j2 < 8; j2++) {
+                const int b2 = j2 < 4 ? j2 : j2 + 4;
+                if (tj ^ ((t1 >> b2) & 1)) athr1 += sw[pj * N + tile_phys(b2, l, a)];
+            }
+            const WT w0 = sw[pj * N + tile_phys(4, l, a)], w1 = sw[pj * N + tile_phys(5, l, a)];
+            const WT w2 = sw[pj * N + tile_phys(6, l, a)], w3 = sw[pj * N + tile_phys(7, l, a)];
+            if (tj) {
+                athr1 += w0 + w1 + w2 + w3;
+                e0 -= w0;
+                e1 -= w1;
+                e2 -= w2;
+                e3 -= w3;
+            } else {
+                e0 += w0;
+                e1 += w1;
+                e2 += w2;
+                e3 += w3;
+            }
+        }
+    }
     i64 thr_off = 0, thr_off1 = 0;
     for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    {
-        const int t1 = lay_index<1>(tid, 0);
-        for (int j = 0; j < kTileBits; j++)
-            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
-    }
+    for (int jj = 0; jj < kTileBits; jj++)
+        if ((t1 >> jj) & 1) thr_off1 |= 1ll << tile_phys(jj, l, a);
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double acc = 0, comp = 0;
@@ -227,7 +265,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
 
     for (; j < my_tiles; j++) {
         const i64 T = blockIdx.x + j * (i64)gridDim.x;
-        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        const i64 base = (tile_mid(T, nmid, A.trot) << l) | ((T >> nmid) << (a + kTileBits - l));
         const int s = (int)(j % kStages);
         double2* buf = stage + (size_t)s * kTile;
         __syncthreads();  // tile j-1 is finished: its stage may be refilled
@@ -305,7 +343,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 }
             }
         }
-        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE) ? 1 : 0;
+        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && (EX == EX_NONE || E1)) ? 1 : 0;
         if (GM != GM_NONE) {
             rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
             if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
@@ -322,10 +360,24 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             }
         }
         if (EX == EX_ENERGY) {
+            const WT* cg = creg;
+            if (E1) {  // cut constants of layout L1
+                cbase = ke[0] + athr1;
+#pragma unroll
+                for (int jj = 0; jj < 8; jj++) {
+                    const int bj = jj < 4 ? jj : jj + 4;
+                    if ((t1 >> bj) & 1) cbase += ke[1 + bj];
+                }
+                g0 = e0 + ke[5];
+                g1 = e1 + ke[6];
+                g2 = e2 + ke[7];
+                g3 = e3 + ke[8];
+                cg = creg1;
+            }
             double ts = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + cg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
             }
