@@ -257,16 +257,6 @@ static int prefetch_distance() {
     return d;
 }
 
-// Rotation of the tile order of the passes (tile_mid; FQ_TROT, 0 = none).
-static int tile_rotation() {
-    static int r = -1;
-    if (r < 0) {
-        const char* e = getenv("FQ_TROT");
-        r = e ? std::max(0, std::min(30, atoi(e))) : 0;
-    }
-    return r;
-}
-
 PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     PassArgs A;
     memset(&A, 0, sizeof(A));
@@ -286,7 +276,6 @@ PassArgs base_args(fq_ctx* ctx, void* sv, int N, const GraphPrep& g) {
     A.W = g.integer ? (double)g.W_int : g.W;
     A.scale = 1.0;
     A.pf_dist = prefetch_distance();
-    A.trot = tile_rotation();
     A.err = ctx->d_err;
     return A;
 }

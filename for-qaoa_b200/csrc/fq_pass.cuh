@@ -98,21 +98,10 @@ struct PassArgs {
                      // the factor (f^2) it gains with every reduced rotation
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
-    int trot;        // tile order: rotation of the fixed bits below the high tile bits (tile_mid)
     int* err;        // device error flag (bounded waits that gave up)
 };
 
 __device__ __forceinline__ int tile_phys(int j, int l, int a) { return j < l ? j : a + j - l; }
-
-// The nmid fixed bits of tile number T that lie between the row bits and the
-// high tile bits, rotated left by rot (none unless 0 < rot < nmid): tiles
-// with consecutive numbers -- the ones the CTAs of a grid work on at the
-// same moment -- then differ in higher address bits.  A bijection on the
-// tiles of a pass, so any rotation visits each tile once.
-__device__ __forceinline__ i64 tile_mid(i64 T, int nmid, int rot) {
-    const i64 mask = (1ll << nmid) - 1, m = T & mask;
-    return (rot > 0 && rot < nmid) ? (((m << rot) | (m >> (nmid - rot))) & mask) : m;
-}
 
 constexpr int kPhaseLo = 32;     // low-part entries of the two-level phase table
 constexpr int kPhaseHiMax = 512; // high-part entries kept in shared memory at most

@@ -96,13 +96,23 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map,
 // 16-byte chunk bits 0..2 are XORed with the 128-byte row bits 0..2.
 __device__ __forceinline__ int tslot(int t) { return t ^ ((t >> 3) & 7); }
 
-// Shared-memory bytes of the TMA pass (1 KB of alignment slack included).
+// Bytes of the cut tables of a TMA pass: PassSmem without its exchange
+// buffer (the landed stage serves as one); FP64 weights need no phase table
+// (sincos), which keeps the ring plus tables within 227 KB.
 template <typename WT>
-__host__ __device__ inline size_t tma_pass_smem_bytes(int N) {
-    return 1024 + (size_t)kStages * kTileBytes + 64 + sizeof(double) * 8 + sizeof(i64) * 32 +
-           sizeof(int) * 24 + sizeof(WT) * (N * N + 32 + 16 + 24 + 16 + 16) + 16 +
-           (sizeof(WT) == sizeof(int) ? phase_smem_bytes() : 0);
+__host__ __device__ constexpr size_t cut_table_bytes() {
+    return sizeof(WT) == sizeof(int) ? PassSmem<WT>::bytes : PassSmem<WT>::smtab;
 }
+
+// Shared-memory bytes of the TMA pass (1 KB of alignment slack included):
+// the ring, the mbarriers, 32 register-slot offsets, the cut tables.
+template <typename WT>
+__host__ __device__ constexpr size_t tma_pass_smem_bytes(int = 0) {
+    return 1024 + (size_t)kStages * kTileBytes + 64 + 32 * sizeof(i64) + cut_table_bytes<WT>();
+}
+static_assert(tma_pass_smem_bytes<int>() <= 227 * 1024, "ring + tables fit one SM (int)");
+static_assert(tma_pass_smem_bytes<double>() <= 227 * 1024, "ring + tables fit one SM (FP64)");
+static_assert(kMaxQubits * kMaxQubits * sizeof(double) <= kTileBytes, "weights fit one stage");
 
 template <typename WT, int PH, int GM, int EX, int SC>
 __global__ void __launch_bounds__(kPassThreads, 1)
@@ -113,20 +123,15 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     double2* stage = reinterpret_cast<double2*>(sm);
     unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + kStages * kTileBytes);
     int* s_abort = reinterpret_cast<int*>(full + kStages);
-    double* red = reinterpret_cast<double*>(full + 8);
-    i64* offtab = reinterpret_cast<i64*>(red + 8);
-    int* fpos = reinterpret_cast<int*>(offtab + 32);
-    WT* sw = reinterpret_cast<WT*>(fpos + 24);
-    WT* ke = sw + A.N * A.N;
-    WT* creg = ke + 32;
-    WT* Dm = creg + 16;
-    WT* Ru = Dm + 24;
-    WT* creg1 = Ru + 16;  // register-bit cut table of layout L1 (E1)
-    double2* smtab = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(creg1 + 16) + 15) & ~(uintptr_t)15);
+    i64* offtab = reinterpret_cast<i64*>(sm + kStages * kTileBytes + 64);
+    unsigned char* tsm = sm + kStages * kTileBytes + 64 + 32 * sizeof(i64);
+    const CutTables<WT> ct(tsm);
+    double* red = reinterpret_cast<double*>(tsm + PassSmem<WT>::red);
+    double2* smtab = reinterpret_cast<double2*>(tsm + PassSmem<WT>::smtab);
     constexpr bool CUT = (PH != PH_NONE) || (EX == EX_ENERGY);
-    // <C> of a pass whose rounds end in layout L1 is taken there (constants
-    // of L1), so the tile leaves from L1 without a change back to L0.
+    constexpr bool INTW = sizeof(WT) == sizeof(int);
+    // <C> of a pass whose rounds end in layout L1 is taken there (the cut
+    // constants of L1), so the tile leaves from L1 without a change back.
     constexpr bool E1 = EX == EX_ENERGY && GM != GM_NONE && SC != SC_L0;
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
@@ -144,14 +149,16 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         if (G.kind == TG_CONTIG) {
             tma_load_3d(dst, &tmap, &full[s], 0, 0, (int)(2 * T));
         } else if (G.kind == TG_ROWS) {
-            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)tile_mid(T, nmid, A.trot), 0,
+            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)(T & ((1ll << nmid) - 1)), 0,
                         (int)(T >> nmid));
         } else {
-            tma_load_5d(dst, &tmap, &full[s], 0, (int)tile_mid(T, nmid, A.trot), 0, 0,
+            tma_load_5d(dst, &tmap, &full[s], 0, (int)(T & ((1ll << nmid) - 1)), 0, 0,
                         (int)(T >> nmid));
         }
     };
 
+    // ---- set-up.  The weights are staged in the last stage, which no copy
+    // fills before the loop's first barrier.
     if (tid == 0) {
         for (int s = 0; s < kStages; s++) mbar_init(&full[s], 1);
         *s_abort = 0;
@@ -164,163 +171,61 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
         offtab[tid] = o;
     }
+    WT* sw = reinterpret_cast<WT*>(stage + (size_t)(kStages - 1) * kTile);
     if (CUT) {
         const WT* gw = reinterpret_cast<const WT*>(A.w);
         for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
-        if (tid < nF) fpos[tid] = tid < nmid ? l + tid : a + (kTileBits - l) + (tid - nmid);
     }
-    if (PH != PH_NONE && sizeof(WT) == sizeof(int)) load_phase_tables(A, smtab, tid, kPassThreads);
+    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, tid, kPassThreads);
     __syncthreads();
     if (tid == 0)
         for (i64 j = 0; j < kStages - 1 && j < my_tiles; j++) issue(j);
-    if (CUT) {
-        if (tid < nF) {
-            const int m = fpos[tid];
-            WT d = 0;
-            for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
-            Dm[tid] = d;
-        } else if (tid >= 32 && tid < 32 + kTileBits) {
-            const int u = tile_phys(tid - 32, l, a);
-            WT r = 0;
-            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
-            Ru[tid - 32] = r;
-        } else if (tid >= 64 && tid < 80) {
-            const int r = tid - 64;
-            WT c = 0;
-            for (int k = 0; k < 4; k++)
-                for (int k2 = k + 1; k2 < 4; k2++)
-                    if (((r >> k) ^ (r >> k2)) & 1)
-                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
-            creg[r] = c;
-        } else if (E1 && tid >= 96 && tid < 112) {
-            const int r = tid - 96;
-            WT c = 0;
-            for (int k = 0; k < 4; k++)
-                for (int k2 = k + 1; k2 < 4; k2++)
-                    if (((r >> k) ^ (r >> k2)) & 1)
-                        c += sw[tile_phys(4 + k, l, a) * N + tile_phys(4 + k2, l, a)];
-            creg1[r] = c;
-        }
-    }
-    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
-    if (CUT) {
-        for (int j = 0; j < 8; j++) {
-            const int pj = tile_phys(j, l, a);
-            const int tj = (tid >> j) & 1;
-            for (int j2 = j + 1; j2 < 8; j2++)
-                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
-            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
-            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
-            if (tj) {
-                athr += w0 + w1 + w2 + w3;
-                f0 -= w0;
-                f1 -= w1;
-                f2 -= w2;
-                f3 -= w3;
-            } else {
-                f0 += w0;
-                f1 += w1;
-                f2 += w2;
-                f3 += w3;
-            }
-        }
-    }
-    // The same per-thread constants for layout L1: thread bits 0..3 and
-    // 8..11 of slot 0's tile index, register bits 4..7.
-    const int t1 = lay_index<1>(tid, 0);
-    WT athr1 = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
-    if (E1) {
-        for (int jj = 0; jj < 8; jj++) {
-            const int bj = jj < 4 ? jj : jj + 4;
-            const int pj = tile_phys(bj, l, a);
-            const int tj = (t1 >> bj) & 1;
-            for (int j2 = jj + 1; j2 < 8; j2++) {
-                const int b2 = j2 < 4 ? j2 : j2 + 4;
-                if (tj ^ ((t1 >> b2) & 1)) athr1 += sw[pj * N + tile_phys(b2, l, a)];
-            }
-            const WT w0 = sw[pj * N + tile_phys(4, l, a)], w1 = sw[pj * N + tile_phys(5, l, a)];
-            const WT w2 = sw[pj * N + tile_phys(6, l, a)], w3 = sw[pj * N + tile_phys(7, l, a)];
-            if (tj) {
-                athr1 += w0 + w1 + w2 + w3;
-                e0 -= w0;
-                e1 -= w1;
-                e2 -= w2;
-                e3 -= w3;
-            } else {
-                e0 += w0;
-                e1 += w1;
-                e2 += w2;
-                e3 += w3;
-            }
-        }
-    }
+    if (CUT) ct.template setup<false>(sw, N, l, a, tid, A.gamma);
+
     i64 thr_off = 0, thr_off1 = 0;
-    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    for (int jj = 0; jj < kTileBits; jj++)
-        if ((t1 >> jj) & 1) thr_off1 |= 1ll << tile_phys(jj, l, a);
+    for (int jj = 0; jj < 8; jj++) thr_off |= (i64)((tid >> jj) & 1) << tile_phys(jj, l, a);
+    {
+        const int t1 = lay_index<1>(tid, 0);
+        for (int jj = 0; jj < kTileBits; jj++)
+            if ((t1 >> jj) & 1) thr_off1 |= 1ll << tile_phys(jj, l, a);
+    }
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
+    WT* const kp = ct.ke;  // written after a tile's first barrier, read after its second
     double acc = 0, comp = 0;
     i64 j = 0;
 
     for (; j < my_tiles; j++) {
         const i64 T = blockIdx.x + j * (i64)gridDim.x;
-        const i64 base = (tile_mid(T, nmid, A.trot) << l) | ((T >> nmid) << (a + kTileBits - l));
+        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
         const int s = (int)(j % kStages);
         double2* buf = stage + (size_t)s * kTile;
-        __syncthreads();  // tile j-1 is finished: its stage may be refilled
+        __syncthreads();  // tile j-1 (or the set-up) is finished: its stage may be refilled
         if (tid == 0 && j + kStages - 1 < my_tiles) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue(j + kStages - 1);
         }
-        if (CUT && warp == 0) {
-            WT h = 0;
-            if (lane < nF) {
-                const int m = fpos[lane];
-                const int zm = (int)((base >> m) & 1);
-                if (zm) h += Dm[lane];
-                for (int i = lane + 1; i < nF; i++)
-                    if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-            if (lane < kTileBits) {
-                const int u = tile_phys(lane, l, a);
-                WT e = Ru[lane];
-                for (int i = 0; i < nF; i++)
-                    if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
-                ke[1 + lane] = e;
-            }
-            if (lane == 0) ke[0] = h;
-        }
+        if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // warps 0 and 1, while the copy lands
         if (!mbar_wait_bounded(&full[s], (unsigned)((j / kStages) & 1))) {
             *s_abort = 1;
             if (A.err) atomicExch(A.err, 1);
         }
-        __syncthreads();  // tile landed (or abort), ke visible
+        __syncthreads();  // tile landed (or abort), kp visible
         if (*s_abort) break;
 
         double2 v[kRegs];
 #pragma unroll
         for (int r = 0; r < kRegs; r++) v[r] = buf[tslot(lay_index<0>(tid, r))];
-        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
-        if (CUT) {
-            cbase = ke[0] + athr;
-#pragma unroll
-            for (int jj = 0; jj < 8; jj++)
-                if ((tid >> jj) & 1) cbase += ke[1 + jj];
-            g0 = f0 + ke[9];
-            g1 = f1 + ke[10];
-            g2 = f2 + ke[11];
-            g3 = f3 + ke[12];
-        }
         if (PH != PH_NONE) {
+            WT cbase, g0, g1, g2, g3;
+            ct.consts(kp, tid, cbase, g0, g1, g2, g3);
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
-                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) +
+                              ((r & 2) ? g1 : WT(0)) + ((r & 4) ? g2 : WT(0)) +
+                              ((r & 8) ? g3 : WT(0));
                 double2 ph;
-                if (sizeof(WT) == sizeof(int)) {
+                if (INTW) {
                     ph = int_phase(A, smtab, (int)cr);
                 } else {
                     const double S = 2.0 * (double)cr - A.W;
@@ -333,7 +238,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                     v[r].x = ph.x * A.scale;
                     v[r].y = ph.y * A.scale;
                 } else {
-                    if (sizeof(WT) != sizeof(int)) {
+                    if (!INTW) {
                         ph.x *= A.scale;
                         ph.y *= A.scale;
                     }
@@ -360,24 +265,14 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             }
         }
         if (EX == EX_ENERGY) {
-            const WT* cg = creg;
-            if (E1) {  // cut constants of layout L1
-                cbase = ke[0] + athr1;
-#pragma unroll
-                for (int jj = 0; jj < 8; jj++) {
-                    const int bj = jj < 4 ? jj : jj + 4;
-                    if ((t1 >> bj) & 1) cbase += ke[1 + bj];
-                }
-                g0 = e0 + ke[5];
-                g1 = e1 + ke[6];
-                g2 = e2 + ke[7];
-                g3 = e3 + ke[8];
-                cg = creg1;
-            }
+            constexpr int LE = E1 ? 1 : 0;  // layout of the registers here
+            WT cbase, g0, g1, g2, g3;
+            ct.template consts<LE>(kp, tid, cbase, g0, g1, g2, g3);
+            const WT* crg = ct.creg + 16 * LE;
             double ts = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + cg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
             }

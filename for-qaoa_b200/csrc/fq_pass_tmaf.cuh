@@ -16,21 +16,12 @@
 
 namespace fq {
 
-// Bytes of the cut tables: PassSmem without its exchange buffer; FP64
-// weights need no phase table (sincos), which keeps the ring plus tables
-// within 227 KB.
-template <typename WT>
-__host__ __device__ constexpr size_t tmaf_table_bytes() {
-    return sizeof(WT) == sizeof(int) ? PassSmem<WT>::bytes : PassSmem<WT>::smtab;
-}
-
+// Shared memory: 1 KB of alignment slack, the ring, the mbarriers, the cut
+// tables (cut_table_bytes).
 template <typename WT>
 __host__ __device__ constexpr size_t tmaf_smem_bytes() {
-    return 1024 + (size_t)kStages * kTileBytes + 64 + tmaf_table_bytes<WT>();
+    return 1024 + (size_t)kStages * kTileBytes + 64 + cut_table_bytes<WT>();
 }
-static_assert(tmaf_smem_bytes<int>() <= 227 * 1024, "ring + tables fit one SM (int)");
-static_assert(tmaf_smem_bytes<double>() <= 227 * 1024, "ring + tables fit one SM (FP64)");
-static_assert(kMaxQubits * kMaxQubits * sizeof(double) <= kTileBytes, "weights fit one stage");
 
 template <typename WT, int GM, int GM2, int SC>
 __global__ void __launch_bounds__(kPassThreads, 1)

@@ -4,8 +4,8 @@ the one-group TMA pass for every read-write sweep (3), with and without the
 L2 prefetch, the strided passes as the warp-specialised pipeline with TMA
 stores (FQ_WS=1) or the one-group TMA pass (FQ_WS=0, the default), the
 fused two-layer schedule (FQ_FUSE=1, the default) or one sweep per pass,
-the fused passes as TMA pipelines (FQ_TMAF=2 all, 1 the strided ones, 0
-none, the default), and rotated tile orders (FQ_TROT).
+and the fused passes as TMA pipelines (FQ_TMAF=2 all, 1 the strided ones,
+0 none, the default).
 The mode is read once per process, so each runs in a child process; states and <C> are checked against the oracle."""
 import json
 import os
@@ -50,15 +50,15 @@ def cases():
     return out
 
 
-@pytest.mark.parametrize("tma,prefetch,ws,fuse,tmaf,trot", [
-    ("0", "0", "1", "1", "1", "0"), ("1", "1", "1", "1", "1", "0"), ("1", "1", "0", "1", "1", "3"),
-    ("2", "0", "1", "1", "0", "0"), ("3", "1", "1", "1", "0", "2"), ("1", "1", "0", "0", "0", "0"),
-    ("0", "0", "0", "0", "0", "0"), ("1", "1", "0", "1", "0", "0"), ("1", "1", "0", "1", "2", "5"),
+@pytest.mark.parametrize("tma,prefetch,ws,fuse,tmaf", [
+    ("0", "0", "1", "1", "1"), ("1", "1", "1", "1", "1"), ("1", "1", "0", "1", "1"),
+    ("2", "0", "1", "1", "0"), ("3", "1", "1", "1", "0"), ("1", "1", "0", "0", "0"),
+    ("0", "0", "0", "0", "0"), ("1", "1", "0", "1", "0"), ("1", "1", "0", "1", "2"),
 ])
-def test_pass_modes_match_oracle(oracle, tma, prefetch, ws, fuse, tmaf, trot):
+def test_pass_modes_match_oracle(oracle, tma, prefetch, ws, fuse, tmaf):
     cs = cases()
     env = dict(os.environ, FQ_TMA=tma, FQ_PREFETCH=prefetch, FQ_WS=ws, FQ_FUSE=fuse,
-               FQ_TMAF=tmaf, FQ_TROT=trot)
+               FQ_TMAF=tmaf)
     res = subprocess.run([sys.executable, "-c", CHILD % {"pkg": PKG}], input=json.dumps(cs),
                          capture_output=True, text=True, env=env, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
