@@ -224,9 +224,18 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic_per_launch(kind):
+def is_headline(args):
+    """Whether the run is the configuration the reference's figure and the
+    committed ncu traffic are quoted on (N=30, p=5)."""
+    return args.n == 30 and args.p == 5
+
+
+def ncu_traffic_per_launch(kind, args):
     """DRAM bytes (read + write) per launch of a pass kind at N=30 from the
-    committed ncu summary (profiles/pass_kernels_n30_p5.md), or None."""
+    committed ncu summary (profiles/pass_kernels_n30_p5.md), or None (other
+    sizes have no committed figure)."""
+    if not is_headline(args):
+        return None
     p = os.path.join(ROOT, "profiles", "pass_kernels_n30_p5.md")
     try:
         m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % kind, open(p).read())
@@ -280,7 +289,7 @@ def run_reference_impl(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_layer * args.p,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": value / BASELINE_LAYERS_PER_S,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(args), "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": "each step: one layer's work units on a 2^%d-amplitude "
@@ -363,7 +372,7 @@ def run_ours(args):
             kern[kind] = {"launches": kn, "ms_avg": kms / kn,
                           "alg_bytes_per_launch": kb / kn, "gbs": kb / (kms / 1000.0) / 1e9,
                           "frac": kb / (kms / 1000.0) / 1e9 / peak,
-                          "traffic": ncu_traffic_per_launch(kind)}
+                          "traffic": ncu_traffic_per_launch(kind, args)}
             tot_ms += kms
             tot_b += kb
             tot_n += kn
@@ -387,7 +396,7 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": value / BASELINE_LAYERS_PER_S,
+        "scaling": "weak", "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(args),
         "parallelism": "replicas" if d.world > 1 else "single",
         "amp_updates_per_s": value * (1 << args.n) * (args.n + 1),
