@@ -106,7 +106,10 @@ inline bool ws_enabled() {
 inline bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G) {
     auto enc = tmap_encoder();
     if (!enc || !A.sv || ((uintptr_t)A.sv & 127) != 0) return false;
-    const int N = A.N, l = A.l, a = A.a, k = kTileBits - l;
+    // The tensor spans the amplitudes in A.sv: 2^12 per tile (A.N can be
+    // larger for a shard of a bigger state, see PassArgs::goff).
+    const int N = kTileBits + __builtin_ctzll((unsigned long long)A.ntiles);
+    const int l = A.l, a = A.a, k = kTileBits - l;
     cuuint64_t dims[5];
     cuuint64_t strides[4];
     cuuint32_t box[5];

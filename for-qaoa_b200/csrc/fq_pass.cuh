@@ -98,6 +98,7 @@ struct PassArgs {
                      // the factor (f^2) it gains with every reduced rotation
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
+    i64 goff;        // shard of a larger state: global index of sv[0] (enters cut values only)
     int* err;        // device error flag (bounded waits that gave up)
 };
 
@@ -578,7 +579,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
         WT* const kp = ct.ke + 32 * par;  // double-buffered: no barrier for the previous readers
         WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
         if (CUT) {
-            ct.tile(kp, base, nF, l, a, warp, lane);
+            ct.tile(kp, base | A.goff, nF, l, a, warp, lane);
             __syncthreads();
             ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }

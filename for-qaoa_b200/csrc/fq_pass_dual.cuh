@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             }
         }
         WT* const kp = ct.ke + 32 * par;
-        if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // read after the exchanges' barriers
+        if (CUT) ct.tile(kp, base | A.goff, nF, l, a, warp, lane);  // read after the exchanges' barriers
         // The thread index re-read in every tile: the exchange addresses
         // derived from it are recomputed (a few integer ops) instead of being
         // hoisted out of the loop, where they would take registers.

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             issue(j + kStages - 1);
         }
-        if (CUT) ct.tile(kp, base, nF, l, a, warp, lane);  // warps 0 and 1, while the copy lands
+        if (CUT) ct.tile(kp, base | A.goff, nF, l, a, warp, lane);  // warps 0 and 1, while the copy lands
         if (!mbar_wait_bounded(&full[s], (unsigned)((j / kStages) & 1))) {
             *s_abort = 1;
             if (A.err) atomicExch(A.err, 1);

@@ -57,6 +57,8 @@ SIGNATURES = {
     "fq_rx_targets": (_i, [_vp, _vp, _i, _ip, _i, _d]),
     "fq_swap_blocks": (_i, [_vp, _vp, _i, _i, _i, _i]),
     "fq_relabel_graph": (_i, [_dp, _i, _i, _i, _i]),
+    "fq_shard_layer": (_i, [_vp, _vp, _i, _i, _i, _dp, _d, _d, _i]),
+    "fq_shard_expectation": (_i, [_vp, _vp, _i, _i, _i, _dp, _dp]),
     "fq_qaoa_forward": (_i, [_vp, _vp, _i, _i, _dp, _dp, _dp, _dp]),
     "fq_expectation": (_i, [_vp, _vp, _i, _dp, _dp]),
     "fq_qaoa_energy_grad": (_i, [_vp, _vp, _vp, _i, _i, _dp, _dp, _dp, _dp, _dp, _dp]),
@@ -258,6 +260,28 @@ class Context:
     def rx_targets(self, st, targets, angle):
         t = np.ascontiguousarray(targets, dtype=np.int32)
         _check(_lib.fq_rx_targets(self.handle, st.ptr, st.n, _iptr(t), len(t), angle),
+               "fq_rx_targets")
+
+    # -- shards of a state split over 2^D devices (raw device pointers) ------
+    def shard_layer(self, ptr, N, D, rank, graph, gamma, beta, first_layer):
+        """Cost phase + RX(beta) on the local qubits of shard `rank`
+        (fq_shard_layer); graph in the shards' current physical order."""
+        g = _f64(graph)
+        _check(_lib.fq_shard_layer(self.handle, _vp(ptr), N, D, rank, _dptr(g), gamma, beta,
+                                   int(bool(first_layer))), "fq_shard_layer")
+
+    def shard_expectation(self, ptr, N, D, rank, graph):
+        """This shard's part of <C> (fq_shard_expectation)."""
+        g = _f64(graph)
+        e = np.zeros(1)
+        _check(_lib.fq_shard_expectation(self.handle, _vp(ptr), N, D, rank, _dptr(g), _dptr(e)),
+               "fq_shard_expectation")
+        return float(e[0])
+
+    def rx_targets_ptr(self, ptr, n, targets, angle):
+        """fq_rx_targets on the 2^n amplitudes at device address ptr."""
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        _check(_lib.fq_rx_targets(self.handle, _vp(ptr), n, _iptr(t), len(t), angle),
                "fq_rx_targets")
 
     def swap_blocks(self, st, swap_out, swap_in, k):

@@ -1,0 +1,188 @@
+#!/usr/bin/env python3
+"""QAOA on a state split over 2^D GPUs (the reference's D > 0 path), one
+process per GPU over torch.distributed (NCCL).
+
+The state of N qubits is split by its top D index bits: rank r holds the
+2^(N-D) amplitudes whose physical qubits N-D..N-1 read r.  One layer:
+
+  1. every rank: cost phase + RX(beta) on its N-D local qubits
+     (fq_shard_layer: the tile passes of the single-GPU engine, with the
+     rank's bits entering the cut values);
+  2. one all-to-all of equal chunks: chunk d of every shard (the amplitudes
+     whose local qubits N-2D..N-D-1 read d) goes to rank d, stored at the
+     position of its source rank.  This swaps qubit blocks [N-2D, N-D) and
+     [N-D, N) -- the reference's global/local swap (src/swap.cu:223-345),
+     here with no packing kernel because the chunks are contiguous;
+  3. every rank: RX(beta) on qubits N-2D..N-D-1, which now hold the qubits
+     that were global (fq_rx_targets);
+  4. the graph is relabelled for the new physical order (fq_relabel_graph,
+     as mapping_after_swap_conti, src/swap.cu:27-50) and the label map
+     records which logical qubit each physical position holds.
+
+The schedule (`forward`) is written against a small interface (`ShardOps`
+methods and an exchange callable), so it runs with one shard per process
+(`dist_exchange`) or with every shard in one process (`local_exchange`).
+
+    torchrun --nproc-per-node 2 --master-addr 127.0.0.1 for-qaoa_b200/sharded.py --n 31 --p 3
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+
+class ShardOps:
+    """One shard on one GPU: a buffer of 2^(N-D) amplitudes, a spare buffer
+    of the same size for the all-to-all, and the CUDA passes of the C ABI.
+    `ctx` must run on the current torch stream, where the exchanges run (a
+    stream of its own, not the legacy default stream, whose handle 0 would
+    give the context a private stream: `shard_context`)."""
+
+    def __init__(self, ctx, N, D, rank, device):
+        import torch
+        cur = torch.cuda.current_stream().cuda_stream
+        if not cur or (ctx.stream or 0) != cur:
+            raise ValueError("the context must run on the current torch stream (shard_context)")
+        self.ctx, self.N, self.D, self.rank = ctx, N, D, rank
+        self.n = N - D
+        self.buf = torch.empty(1 << self.n, dtype=torch.complex128, device=device)
+        self.spare = torch.empty_like(self.buf)
+
+    def layer(self, graph, gamma, beta, first_layer):
+        self.ctx.shard_layer(self.buf.data_ptr(), self.N, self.D, self.rank, graph, gamma, beta,
+                             first_layer)
+
+    def rx_top(self, beta):
+        n, D = self.n, self.D
+        self.ctx.rx_targets_ptr(self.buf.data_ptr(), n, list(range(n - D, n)), beta)
+
+    def expectation(self, graph):
+        return self.ctx.shard_expectation(self.buf.data_ptr(), self.N, self.D, self.rank, graph)
+
+    def swap(self):
+        self.buf, self.spare = self.spare, self.buf
+
+
+def shard_context(device):
+    """A torch stream made current on `device` and a library context on it,
+    so the passes and the exchanges share one stream order.  Returns
+    (stream, context); the caller closes the context."""
+    import torch
+    import forqaoa
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+    return stream, forqaoa.Context(device, stream.cuda_stream)
+
+
+def local_exchange(shards):
+    """The all-to-all with every shard in this process (shards[r] is rank
+    r's): shard d receives chunk d of every shard r at chunk position r."""
+    R = len(shards)
+    m = shards[0].buf.numel() // R
+    for d, sd in enumerate(shards):
+        for r, sr in enumerate(shards):
+            sd.spare[r * m:(r + 1) * m].copy_(sr.buf[d * m:(d + 1) * m])
+    for s in shards:
+        s.swap()
+
+
+def dist_exchange(shards):
+    """The all-to-all with one shard per process over torch.distributed
+    (NCCL on GPUs, in the current stream's order; gloo on CPU tensors),
+    equal splits."""
+    import torch
+    import torch.distributed as dist
+    (s,) = shards
+    dist.all_to_all_single(torch.view_as_real(s.spare), torch.view_as_real(s.buf))
+    s.swap()
+
+
+def relabel(graph, swap_out, swap_in, k):
+    import forqaoa
+    return forqaoa.relabel_graph(graph, swap_out, swap_in, k)
+
+
+def forward(shards, exchange, N, D, graph, gammas, betas, relabel_fn=relabel):
+    """The P-layer circuit from |+>^N on the given shards.  Returns the
+    label map (physical position -> logical qubit) and the graph in the
+    final physical order."""
+    n = N - D
+    labels = np.arange(N)
+    g = np.ascontiguousarray(graph, dtype=np.float64)
+    for p, (gamma, beta) in enumerate(zip(gammas, betas)):
+        for s in shards:
+            s.layer(g, gamma, beta, p == 0)
+        exchange(shards)
+        for s in shards:
+            s.rx_top(beta)
+        g = relabel_fn(g, n - D, n, D)
+        labels[n - D:n], labels[n:N] = labels[n:N].copy(), labels[n - D:n].copy()
+    return labels, g
+
+
+def to_logical(state_phys, labels):
+    """Reorder a gathered physical-order state: position b holds logical
+    qubit labels[b]."""
+    N = len(labels)
+    y = np.arange(1 << N, dtype=np.int64)
+    x = np.zeros_like(y)
+    for b, q in enumerate(labels):
+        x |= ((y >> b) & 1) << int(q)
+    out = np.empty_like(state_phys)
+    out[x] = state_phys
+    return out
+
+
+def main(argv=None):
+    import torch
+    import torch.distributed as dist
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--n", type=int, default=31)
+    ap.add_argument("--p", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=3)
+    a = ap.parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    D = world.bit_length() - 1
+    if world < 2 or (1 << D) != world:
+        raise SystemExit("needs a power-of-two world size >= 2 (one rank per GPU)")
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import datetime
+    stream, ctx = shard_context(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rng = np.random.default_rng(a.seed)
+    W = np.triu(rng.integers(1, 11, (a.n, a.n)).astype(np.float64), 1)
+    gammas, betas = rng.uniform(0, np.pi, a.p), rng.uniform(0, np.pi / 2, a.p)
+    s = ShardOps(ctx, a.n, D, rank, "cuda")
+    # Device time on the ranks' streams (CUDA events), the max over ranks.
+    times = []
+    for _ in range(a.steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        _, g = forward([s], dist_exchange, a.n, D, W, gammas, betas)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        times.append(t0.elapsed_time(t1) / 1000.0)
+    e = torch.tensor([s.expectation(g)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(e)
+    t = torch.tensor([min(times)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        print(json.dumps({"N": a.n, "D": D, "p": a.p, "ranks": world,
+                          "layers_per_s": a.p / float(t.item()), "energy": float(e.item())}))
+    ctx.close()
+    dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

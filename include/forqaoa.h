@@ -118,6 +118,28 @@ int fq_swap_blocks(fq_ctx* ctx, void* sv, int N, int swap_out, int swap_in,
 int fq_relabel_graph(double* graph_upper, int N, int swap_out, int swap_in,
                      int num_swap);
 
+/* ---- sharded state (D > 0) ------------------------------------------------
+ * A state of N qubits split over 2^D devices by its top D index bits: the
+ * shard of rank r holds the 2^(N-D) amplitudes whose physical qubits
+ * N-D..N-1 read r (N-D >= 13).  graph_upper is the N x N graph in the
+ * shards' current physical order.  A layer is fq_shard_layer on every
+ * shard, then an all-to-all of equal chunks (chunk d of every shard to rank
+ * d; it swaps qubit blocks [N-2D, N-D) and [N-D, N)), then fq_rx_targets on
+ * qubits N-2D..N-D-1 of every shard and fq_relabel_graph(graph, N, N-2D,
+ * N-D, D); for-qaoa_b200/sharded.py drives it over torch.distributed.
+ * Replaces the D > 0 paths of rotationCompressionWeighted, multiRotateX and
+ * swap_gate_conti (src/rzz.cu:173-206, src/rx.cu:118-174,
+ * src/swap.cu:104-165,223-345). */
+/* Cost phase of angle gamma (first_layer != 0: launch-control init with
+ * fq_init_amp(N), the shard is written without being read) followed by
+ * RX(beta) on the shard's local qubits 0..N-D-1. */
+int fq_shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank,
+                   const double* graph_upper, double gamma, double beta, int first_layer);
+/* <C> summed over this shard's amplitudes (the shards' partials add up to
+ * <C>); synchronises the stream. */
+int fq_shard_expectation(fq_ctx* ctx, const void* shard, int N, int D, int rank,
+                         const double* graph_upper, double* partial);
+
 /* ---- fused engine --------------------------------------------------------
  * The whole P-layer circuit from |+>^N in as few HBM sweeps as possible:
  * cost phase, launch-control init and the first 12 RX gates share one
