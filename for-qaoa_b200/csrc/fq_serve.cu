@@ -60,6 +60,7 @@ struct Session {
     void* sv = nullptr;
     void* cs = nullptr;
     bool busy = false;
+    bool heavy = false;   // its running step counts against the heavy cap
     bool closed = false;  // release once the running step completes
     int queued = 0;       // its requests waiting for a lane
     double last_used = 0;
@@ -76,6 +77,21 @@ struct Lane {
 constexpr int kBatchCap = 4096;           // small instances per launch
 constexpr int kExpressN = 20;             // lane requests up to this size go first
 constexpr double kEvictIdleS = 0.05;      // a session idle this long may lose its buffers
+constexpr int kHeavyN = 24;               // requests this large fill the GPU on their own
+
+// Requests with N >= kHeavyN in flight at once (FQ_SERVE_HEAVY, 0 = no
+// cap; default 1).  Each one alone keeps HBM busy, so running two together
+// gains no throughput (10,000-request stream on B200: 167 evals/s with the
+// cap, 166 without) and holds the other lanes' short requests back: p50
+// latency 3.5 ms with the cap, 12.9 ms without.
+static int heavy_cap() {
+    static int c = -1;
+    if (c < 0) {
+        const char* e = getenv("FQ_SERVE_HEAVY");
+        c = e ? std::max(0, atoi(e)) : 1;
+    }
+    return c;
+}
 constexpr size_t kBatchBytes = 8u << 20;  // descriptors + data per launch
 constexpr int kBatchOut = kBatchCap * (1 + 2 * FQ_SERVE_MAX_LAYERS);
 
@@ -101,6 +117,7 @@ struct fq_server {
     int device = 0;
     double budget = 0;
     size_t used = 0;  // bytes of resident session buffers
+    int heavy_running = 0;  // steps with N >= kHeavyN on lanes (guarded by mu)
     cudaMemPool_t pool = nullptr;
     cudaStream_t free_stream = nullptr;
     std::vector<Lane> lanes;
@@ -279,6 +296,8 @@ struct fq_server {
             if (it->N > nmax) continue;
             Session& s = sessions[it->session];
             if (s.busy) continue;
+            const bool heavy = it->N >= kHeavyN;
+            if (heavy && heavy_cap() > 0 && heavy_running >= heavy_cap()) continue;
             if (resident_only && !(s.sv && s.N == it->N)) continue;
             if (s.sv && s.N != it->N) drop_buffers(s);  // the session changed size
             if (!s.sv) {
@@ -288,6 +307,8 @@ struct fq_server {
             }
             s.N = it->N;
             s.busy = true;
+            s.heavy = heavy;
+            heavy_running += heavy ? 1 : 0;
             s.queued--;
             s.last_used = now_s();
             out = std::move(*it);
@@ -334,6 +355,8 @@ struct fq_server {
         std::lock_guard<std::mutex> lk(mu);
         auto it = sessions.find(id);
         if (it == sessions.end()) return;
+        if (it->second.heavy) heavy_running--;
+        it->second.heavy = false;
         it->second.busy = false;
         it->second.last_used = now_s();
         if (it->second.closed && it->second.queued == 0) {
