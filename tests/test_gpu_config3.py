@@ -54,3 +54,27 @@ def test_n32_p3_fused_matches_reference_schedule(ctx, config3):
     finally:
         st.free()
     assert abs(e_fused - e_ref) <= ENERGY_RTOL * abs(e_ref), (e_fused, e_ref)
+
+
+def test_n33_max_size_light_cone(ctx, oracle):
+    """The largest state the library takes: N=33 (128 GiB, every one of the
+    21 fixed-bit slots of the cut tables in use), p=2 on a random 3-regular
+    graph with FP64 weights, <C> against the light-cone sum of the oracle;
+    then integer weights (the two-level phase tables), p=1."""
+    rng = np.random.default_rng(33)
+    n = 33
+    edges = random_regular(n - 1, 3, rng) + [(31, 32)]  # vertex 32 joins by one edge
+    W = weighted_graph(n, edges, rng)
+    g, b = rng.uniform(0, np.pi, 2), rng.uniform(0, np.pi / 2, 2)
+    st = ctx.state(n)
+    try:
+        e = ctx.qaoa_forward(st, W, g, b)
+        want = light_cone_energy(oracle, n, edges, W, g, b)
+        assert abs(e - want) <= ENERGY_RTOL * abs(want), (e, want)
+        Wi = np.where(W > 0, rng.integers(1, 10, W.shape), 0).astype(float)
+        g1, b1 = rng.uniform(0, np.pi, 1), rng.uniform(0, np.pi / 2, 1)
+        e = ctx.qaoa_forward(st, Wi, g1, b1)
+        want = light_cone_energy(oracle, n, edges, Wi, g1, b1)
+        assert abs(e - want) <= ENERGY_RTOL * abs(want), (e, want)
+    finally:
+        st.free()
