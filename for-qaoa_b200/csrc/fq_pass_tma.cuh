@@ -26,7 +26,11 @@ namespace fq {
 
 constexpr int kStages = 3;
 constexpr unsigned kTileBytes = kTile * sizeof(double2);  // 64 KB
-constexpr long long kWaitSpins = 1ll << 22;              // bound on mbarrier polls
+// Bound on mbarrier polls: a poll that finds the phase incomplete suspends
+// the thread for ~4 us on B200 (2^16 polls measured 0.26 s), so 2^18 polls
+// give up after about a second; a landing copy ends the wait at once.
+constexpr long long kWaitSpins = 1ll << 18;
+constexpr long long kIssueSpins = 1ll << 22;  // polls of 32 ns sleeps (two-group stage guard)
 
 // Box geometry of a pass (host-chosen, see make_pass_tmap):
 //   TG_CONTIG  l = 12: rank 3, box {16 doubles, 256 rows, 2}
@@ -65,11 +69,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of an mbarrier; false if it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (long long i = 0; i < kWaitSpins; i++)
+// Bounded wait for phase `parity` of an mbarrier: at most max_polls polls
+// (each may suspend the thread for a while); false if it gave up.  A
+// %globaltimer bound in the loop cost the strided pass 10% (7.05 vs 6.41 ms
+// at N=30), so the bound is a poll count.
+__device__ __forceinline__ bool mbar_wait_polls(unsigned long long* bar, unsigned parity,
+                                                long long max_polls) {
+    for (long long i = 0; i < max_polls; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    return mbar_wait_polls(bar, parity, kWaitSpins);
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map,
@@ -491,7 +503,7 @@ __global__ void __launch_bounds__(2 * kPassThreads, 1)
         // j-3's phase, whose parity differs from tile j's, so a parity wait
         // would return at once: wait for the issue first (bounded).
         bool ok = false;
-        for (long long i = 0; i < kWaitSpins; i++) {
+        for (long long i = 0; i < kIssueSpins; i++) {
             if (*(volatile long long*)&issued[s] == j) {
                 ok = true;
                 break;

@@ -40,6 +40,7 @@ SIGNATURES = {
     "fq_ctx_create": (_i, [_i, _vp, ctypes.POINTER(_vp)]),
     "fq_ctx_destroy": (_i, [_vp]),
     "fq_ctx_synchronize": (_i, [_vp]),
+    "fq_ctx_selftest_wait": (_i, [_vp]),
     "fq_ctx_stream": (_vp, [_vp]),
     "fq_ctx_kernel_launches": (_i, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "fq_ctx_device_info": (_i, [_vp, _ip, _ip]),

@@ -54,6 +54,14 @@ int fq_version(void);
 int fq_ctx_create(int device, void* stream, fq_ctx** out);
 int fq_ctx_destroy(fq_ctx* ctx);
 int fq_ctx_synchronize(fq_ctx* ctx);
+/* Self-test of the failure path (no counterpart in the reference, whose
+ * waits are unbounded): enqueues one kernel that waits, with the bounded
+ * wait of the TMA pipelines (2^16 polls instead of 2^18: 0.26 s instead of
+ * about 1 s on B200), on a barrier
+ * nothing completes.  The wait gives up, the next synchronising call (e.g.
+ * fq_ctx_synchronize) returns FQ_ERR_TIMEOUT and clears the flag, and the
+ * context stays usable. */
+int fq_ctx_selftest_wait(fq_ctx* ctx);
 void* fq_ctx_stream(fq_ctx* ctx);
 /* Number of library kernels this context has launched so far. */
 int fq_ctx_kernel_launches(fq_ctx* ctx, long long* count);
