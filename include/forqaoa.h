@@ -129,12 +129,13 @@ int fq_relabel_graph(double* graph_upper, int N, int swap_out, int swap_in,
 /* ---- sharded state (D > 0) ------------------------------------------------
  * A state of N qubits split over 2^D devices by its top D index bits: the
  * shard of rank r holds the 2^(N-D) amplitudes whose physical qubits
- * N-D..N-1 read r (N-D >= 13).  graph_upper is the N x N graph in the
- * shards' current physical order.  A layer is fq_shard_layer on every
- * shard, then an all-to-all of equal chunks (chunk d of every shard to rank
- * d; it swaps qubit blocks [N-2D, N-D) and [N-D, N)), then fq_rx_targets on
- * qubits N-2D..N-D-1 of every shard and fq_relabel_graph(graph, N, N-2D,
- * N-D, D); for-qaoa_b200/sharded.py drives it over torch.distributed.
+ * N-D..N-1 read r (1 <= D <= 8, N-D >= 13, rank < 2^D).  graph_upper is
+ * the N x N graph in the shards' current physical order.  A layer is
+ * fq_shard_layer on every shard, then an all-to-all of equal chunks (chunk
+ * d of every shard to rank d; it swaps qubit blocks [N-2D, N-D) and
+ * [N-D, N)), then fq_rx_targets on qubits N-2D..N-D-1 of every shard and
+ * fq_relabel_graph(graph, N, N-2D, N-D, D); for-qaoa_b200/sharded.py
+ * drives it over torch.distributed.
  * Replaces the D > 0 paths of rotationCompressionWeighted, multiRotateX and
  * swap_gate_conti (src/rzz.cu:173-206, src/rx.cu:118-174,
  * src/swap.cu:104-165,223-345). */
