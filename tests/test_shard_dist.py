@@ -116,3 +116,21 @@ def test_sharded_schedule_matches_oracle(oracle, world, N, P, kind):
     assert abs(e - eo) <= ENERGY_RTOL * max(1.0, abs(eo))
     # Every layer moves D qubits out of and back into the device bits.
     assert sorted(labels.tolist()) == list(range(N))
+
+
+@pytest.mark.parametrize("D,N,P", [(1, 8, 2), (2, 9, 3), (3, 10, 2)])
+def test_local_exchange_schedule_matches_oracle(oracle, D, N, P):
+    """Every shard in this process: `local_exchange` (the chunk copies the
+    one-GPU emulation uses) in place of the collective."""
+    import sharded
+    rng = np.random.default_rng(7 * N + D)
+    W = complete_int(N, rng)
+    g, b = angles(rng, P)
+    shards = [NumpyShard(N, D, r) for r in range(1 << D)]
+    labels, gfin = sharded.forward(shards, sharded.local_exchange, N, D, W, g, b)
+    psi = torch.cat([s.buf for s in shards]).numpy()
+    want = oracle.qaoa_logical(W, g, b)
+    assert_state_close(sharded.to_logical(psi, labels), want, what=f"local N={N} D={D}")
+    e = sum(s.expectation(gfin) for s in shards)
+    eo = oracle.expectation(want, W)
+    assert abs(e - eo) <= ENERGY_RTOL * max(1.0, abs(eo))
