@@ -35,6 +35,24 @@ def test_library_exports_every_declared_symbol(fq):
     assert sorted(fq.SIGNATURES) == declared_functions()
 
 
+def declared_arity():
+    """{name: number of parameters} of every fq_* declaration."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(fq_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_python_bindings_match_declared_arity(fq):
+    arity = declared_arity()
+    assert sorted(arity) == declared_functions()
+    wrong = {n: (len(fq.SIGNATURES[n][1]), k) for n, k in arity.items()
+             if len(fq.SIGNATURES[n][1]) != k}
+    assert not wrong, wrong
+
+
 REFAPI_SYMBOLS = [
     "_Z11createStateiiii", "_Z12destroyStateRK5State", "_Z20stateCpyDeviceToHostRK5State",
     "_Z20stateCpyHostToDeviceRK5State", "_Z20stateInitDeviceStateRK5State",
