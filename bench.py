@@ -290,7 +290,9 @@ def run_reference_impl(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_layer * args.p,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
-        "dtype": "f64", "data": "synthetic", "config": workload_config(args), "impl": "reference",
+        "dtype": "f64", "data": "synthetic",
+        "config": dict(workload_config(args), engine="oracle port on the host cores (FP64, OpenMP)"),
+        "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": "each step: one layer's work units on a 2^%d-amplitude "
                                    "slice, scaled to a full N=%d layer (wall %.1f s for %d "
