@@ -26,6 +26,7 @@ methods and an exchange callable), so it runs with one shard per process
     torchrun --nproc-per-node 2 --master-addr 127.0.0.1 for-qaoa_b200/sharded.py --n 31 --p 3
 """
 import argparse
+import datetime
 import json
 import os
 import sys
@@ -155,7 +156,6 @@ def main(argv=None):
     if world < 2 or (1 << D) != world:
         raise SystemExit("needs a power-of-two world size >= 2 (one rank per GPU)")
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    import datetime
     stream, ctx = shard_context(local)
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     rng = np.random.default_rng(a.seed)
