@@ -24,6 +24,7 @@ methods and an exchange callable), so it runs with one shard per process
 (`dist_exchange`) or with every shard in one process (`local_exchange`).
 
     torchrun --nproc-per-node 2 --master-addr 127.0.0.1 for-qaoa_b200/sharded.py --n 31 --p 3
+    python for-qaoa_b200/sharded.py --n 30 --emulate 1     # both shards on one GPU, timed
 """
 import argparse
 import datetime
@@ -141,6 +142,44 @@ def to_logical(state_phys, labels):
     return out
 
 
+def emulate(n_qubits, D, P, seed):
+    """Every shard on GPU 0 (the exchange as chunk copies): device time per
+    layer of the shard passes, the exchange and the RX of the swapped-in
+    qubits, by CUDA events (the first layer runs untimed as warm-up)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    N = n_qubits
+    W = np.triu(rng.integers(1, 11, (N, N)).astype(np.float64), 1)
+    g, b = rng.uniform(0, np.pi, P), rng.uniform(0, np.pi / 2, P)
+    stream, ctx = shard_context(0)
+    try:
+        shards = [ShardOps(ctx, N, D, r, "cuda") for r in range(1 << D)]
+        forward(shards, local_exchange, N, D, W, g[:1], b[:1])
+        torch.cuda.synchronize()
+        n = N - D
+        gphys = np.ascontiguousarray(W)
+        t = {"shard_passes": 0.0, "exchange": 0.0, "rx_swapped_in": 0.0}
+        for p in range(P):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record(stream)
+            for s in shards:
+                s.layer(gphys, g[p], b[p], p == 0)
+            e[1].record(stream)
+            local_exchange(shards)
+            e[2].record(stream)
+            for s in shards:
+                s.rx_top(b[p])
+            e[3].record(stream)
+            torch.cuda.synchronize()
+            for k, (i, j) in zip(t, ((0, 1), (1, 2), (2, 3))):
+                t[k] += e[i].elapsed_time(e[j])
+            gphys = relabel(gphys, n - D, n, D)
+        return {"N": N, "D": D, "p": P, "shards_on_one_gpu": 1 << D,
+                "ms_per_layer": {k: v / P for k, v in t.items()}}
+    finally:
+        ctx.close()
+
+
 def main(argv=None):
     import torch
     import torch.distributed as dist
@@ -149,7 +188,12 @@ def main(argv=None):
     ap.add_argument("--p", type=int, default=3)
     ap.add_argument("--seed", type=int, default=30)
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--emulate", type=int, default=0, metavar="D",
+                    help="run all 2^D shards on GPU 0 (no torch.distributed) and time the parts")
     a = ap.parse_args(argv)
+    if a.emulate:
+        print(json.dumps(emulate(a.n, a.emulate, a.p, a.seed)))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     D = world.bit_length() - 1
