@@ -18,8 +18,9 @@ Also reported on the same JSON line:
                events on the library's stream), against the measured HBM copy
                bandwidth; per_layer gives the same over every pass of a layer;
   cpu_baseline the oracle (plain FP64 OpenMP restatement of the reference's
-               algorithm) timed on a bounded slice of one layer on the host
-               cores, scaled to a full N=30 layer;
+               algorithm) timed on the host cores on one whole N=30 layer of
+               a full 16 GiB host state, beside the estimate from timed
+               equal parts of a layer (scale_check = full / estimate);
   reference_schedule  the reference's own per-layer schedule (cost sweep, RX
                chunks of C=12, block swaps) through this library's per-kernel
                entry points, with per-kernel HBM GB/s;
@@ -32,7 +33,9 @@ Also reported on the same JSON line:
 
 `--impl reference` times the reference algorithm on the host cores (the
 reference ships no CPU implementation; the oracle port stands in) on the same
-workload and metric, one bounded sample per step.
+workload and metric: each step is one of 32 equal parts of a layer on the
+full-size state (value = parts' share of a layer / their time), and one
+whole layer is timed once at the end as a check of the parts.
 """
 import argparse
 import json
@@ -66,13 +69,18 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=30)
+    ap.add_argument("--n", "--qubits", dest="n", type=int, default=30)
     ap.add_argument("--p", type=int, default=5)
     ap.add_argument("--chunk", type=int, default=12)
     ap.add_argument("--seed", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-ref-schedule", action="store_true")
-    ap.add_argument("--cpu-slice-bits", type=int, default=24)
+    ap.add_argument("--cpu-parts", type=int, default=8,
+                    help="parts (of 32 per layer) timed for the CPU estimate")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA build")
+    ap.add_argument("--no-cpu-full", action="store_true",
+                    help="skip the whole-layer CPU measurement (parts only)")
     ap.add_argument("--serve-requests", type=int, default=1000,
                     help="requests of the served-stream leg (0: skip it)")
     ap.add_argument("--serve-lanes", type=int, default=4)
@@ -94,7 +102,7 @@ def workload_config(args):
                     "(%d GiB)" % (args.n, args.p, args.n, (16 << args.n) >> 30),
         "N": args.n, "p": args.p, "graph": "K%d" % args.n, "weights": "int U{1..10}",
         "angles": "gamma~U[0,pi), beta~U[0,pi/2)", "seed": args.seed,
-        "engine": "fused tile passes", "l2": "state larger than L2 (no flush needed)",
+        "l2": "state larger than L2 (no flush needed)",
     }
 
 
@@ -246,59 +254,126 @@ def ncu_traffic_per_launch(kind, args):
 
 # ------------------------------------------------------------ CPU leg --
 
-def cpu_sample(graph, gamma, beta, slice_bits):
+CPU_CHUNKS = 32
+
+
+def cpu_layer_parts(cl, gammas, betas, parts, start=0):
+    """Seconds of `parts` consecutive parts (1/CPU_CHUNKS of a layer each)."""
+    return [cl.chunk(start + k, gammas[(start + k) % len(gammas)],
+                     betas[(start + k) % len(betas)]) for k in range(parts)]
+
+
+def cpu_baseline_obj(args, graph, gammas, betas):
+    """The oracle on the host cores at the benchmark's size: one whole layer
+    of a full 2^N host state (the value), and the estimate from `cpu_parts`
+    timed parts of a layer (scale_check = whole / estimate)."""
     import oracle
-    tc, tr, full = oracle.layer_sample(graph, slice_bits, gamma, beta)
-    return full, tc + tr, oracle.num_threads()
+    cl = oracle.CpuLayer(graph, CPU_CHUNKS)
+    try:
+        cpu_layer_parts(cl, gammas, betas, 1)  # warm-up part
+        t_parts = cpu_layer_parts(cl, gammas, betas, args.cpu_parts, start=1)
+        est = sum(t_parts) * CPU_CHUNKS / len(t_parts)
+        full = None if args.no_cpu_full else cl.full_layer(gammas[1], betas[1])
+    finally:
+        cl.free()
+    cores = oracle.num_threads()
+    out = {"unit": UNIT, "cores": cores, "kind": "port",
+           "parts_estimate_s": est, "parts_timed": len(t_parts), "parts_per_layer": CPU_CHUNKS}
+    if full is not None:
+        out.update(value=1.0 / full, full_layer_s=full, scale_check=full / est,
+                   sample="oracle (FP64 OpenMP restatement of src/rzz.cu:121-156 and "
+                          "src/rx.cu:32-53) on one whole N=%d layer of a full 2^%d-amplitude "
+                          "host state: the read-multiply cost phase with the K_%d pair loop on "
+                          "every amplitude, then RX on every qubit; value = 1 / its time "
+                          "(measured, not scaled); parts_estimate_s = %d timed parts of 1/%d "
+                          "layer scaled by %d/%d"
+                          % (args.n, args.n, args.n, len(t_parts), CPU_CHUNKS, CPU_CHUNKS,
+                             len(t_parts)))
+    else:
+        out.update(value=1.0 / est,
+                   sample="oracle on %d timed parts of 1/%d of an N=%d layer of a full "
+                          "host state, scaled to a layer" % (len(t_parts), CPU_CHUNKS, args.n))
+    return out
 
 
-def cpu_baseline_obj(args, graph, gamma, beta, reps=2):
-    best = None
-    for _ in range(reps):
-        full, wall, cores = cpu_sample(graph, gamma, beta, args.cpu_slice_bits)
-        best = full if best is None else min(best, full)
-    return {"value": 1.0 / best, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": "oracle (FP64 OpenMP restatement of src/rzz.cu:121-156 and "
-                      "src/rx.cu:32-53) on one layer's work units over a 2^%d-amplitude "
-                      "slice of the N=%d circuit (cost phase with the full K_%d pair loop, "
-                      "RX on the slice's %d qubits), scaled by amplitude and pair-update "
-                      "counts to a full N=%d layer; best of %d"
-                      % (args.cpu_slice_bits, args.n, args.n, args.cpu_slice_bits, args.n,
-                         reps)}
+def reference_gpu_leg(args, graph, gammas, betas, chunk=11):
+    """The reference's own single-device CUDA path (its unmodified sources,
+    built by oracle/Makefile.ref with CHUNK_QUBIT = 11, the chunk of its
+    committed ncu report) on this box's GPU: the layer loop of
+    src/Weighted.cpp:115-138 timed with CUDA events on its compute stream."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(ORACLE_DIR, "_ref", "ref_harness_c%d" % chunk)
+    if not os.path.exists(exe):
+        return {"unavailable": "reference build oracle/_ref/ref_harness_c%d not present" % chunk}
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout, fidx = (os.path.join(td, x) for x in ("in.bin", "out.bin", "idx.bin"))
+        with open(fin, "wb") as f:
+            f.write(np.array([args.n, chunk, len(gammas)], dtype=np.int32).tobytes())
+            f.write(np.ascontiguousarray(graph, dtype=np.float64).tobytes())
+            f.write(np.asarray(gammas, dtype=np.float64).tobytes())
+            f.write(np.asarray(betas, dtype=np.float64).tobytes())
+        np.array([0], dtype=np.int64).tofile(fidx)
+        r = subprocess.run([exe, fin, fout, "sample", fidx], capture_output=True, text=True,
+                           timeout=900)
+        if r.returncode != 0:
+            return {"unavailable": "reference harness exited %d: %s"
+                    % (r.returncode, (r.stderr or r.stdout)[-300:])}
+        raw = np.fromfile(fout, dtype=np.float64)
+    loop_ms, norm, energy = (float(x) for x in raw[:3])
+    return {"layers_per_s": len(gammas) / (loop_ms / 1000.0), "loop_ms": loop_ms,
+            "chunk_qubit": chunk, "layers": len(gammas), "energy": energy, "norm": norm,
+            "how": "FOR-QAOA's unmodified single-device CUDA path (oracle/Makefile.ref, "
+                   "CHUNK_QUBIT=%d) run through oracle/ref_harness.cpp on this GPU; CUDA events "
+                   "on its compute stream around the layer loop (its host-side launch work, "
+                   "graph packing and swap tables included)" % chunk}
 
 
 def run_reference_impl(args):
-    """The reference algorithm on the host cores (oracle port), same metric."""
+    """The reference algorithm on the host cores (oracle port), same metric
+    and workload: each step is one part (1/32) of a layer on the full-size
+    host state; one whole layer is timed once after the steps."""
     d = Dist()
     if d.rank != 0:
         d.close()
         return
+    import oracle
     graphs, gammas, betas = workload(args.n, args.p, args.seed)
-    for _ in range(args.warmup):
-        cpu_sample(graphs[0], gammas[0], betas[0], args.cpu_slice_bits)
-    t_layers = []
     wall0 = time.perf_counter()
-    cores = 1
-    for k in range(args.steps):
-        full, _, cores = cpu_sample(graphs[0], gammas[k % args.p], betas[k % args.p],
-                                    args.cpu_slice_bits)
-        t_layers.append(full)
+    cl = oracle.CpuLayer(graphs[0], CPU_CHUNKS)
+    try:
+        cpu_layer_parts(cl, gammas, betas, args.warmup)
+        t_steps = cpu_layer_parts(cl, gammas, betas, args.steps, start=args.warmup)
+        full = None if args.no_cpu_full else cl.full_layer(gammas[1], betas[1])
+    finally:
+        cl.free()
     wall = time.perf_counter() - wall0
-    ms_layer = 1000.0 * statistics.mean(t_layers)
-    value = 1000.0 / ms_layer
+    ms_step = 1000.0 * statistics.mean(t_steps)
+    value = (1.0 / CPU_CHUNKS) / (ms_step / 1000.0)
+    cores = oracle.num_threads()
+    cpu = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": "each step: part k (of %d) of one N=%d layer on a full 2^%d-amplitude "
+                     "host state -- the read-multiply cost phase with the K_%d pair loop on "
+                     "1/%d of the amplitudes, RX on every qubit for 1/%d of its pairs; value "
+                     "= (1/%d layer) / mean step time; wall %.1f s for the whole run"
+                     % (CPU_CHUNKS, args.n, args.n, args.n, CPU_CHUNKS, CPU_CHUNKS,
+                        CPU_CHUNKS, wall)}
+    if full is not None:
+        cpu.update(full_layer_s=full, scale_check=full / (CPU_CHUNKS * ms_step / 1000.0))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_layer * args.p,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
-        "dtype": "f64", "data": "synthetic",
-        "config": dict(workload_config(args), engine="oracle port on the host cores (FP64, OpenMP)"),
-        "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "each step: one layer's work units on a 2^%d-amplitude "
-                                   "slice, scaled to a full N=%d layer (wall %.1f s for %d "
-                                   "steps)" % (args.cpu_slice_bits, args.n, wall, args.steps)},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+        "engine": "oracle port on the host cores (FP64, OpenMP): the reference ships no CPU "
+                  "implementation",
+        "layers_per_step": 1.0 / CPU_CHUNKS,
+        "impl": "reference", "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_ref_gpu:
+        line["reference_gpu"] = reference_gpu_leg(args, graphs[0], gammas, betas)
     print(json.dumps(line), flush=True)
     d.close()
 
@@ -400,6 +475,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": (value / BASELINE_LAYERS_PER_S) if is_headline(args) else None,
         "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+        "engine": "fused tile passes (fq_qaoa_forward)", "layers_per_step": args.p,
         "parallelism": "replicas" if d.world > 1 else "single",
         "amp_updates_per_s": value * (1 << args.n) * (args.n + 1),
         "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
@@ -419,7 +495,7 @@ def run_ours(args):
         line["serving"] = serving_leg(args)
     # ---- CPU baseline (rank 0, one GPU only)
     if not args.no_cpu and d.world == 1 and d.rank == 0:
-        line["cpu_baseline"] = cpu_baseline_obj(args, graphs[0], gammas[0], betas[0])
+        line["cpu_baseline"] = cpu_baseline_obj(args, graphs[0], gammas, betas)
     ctx.close()
     if d.rank == 0:
         print(json.dumps(line), flush=True)

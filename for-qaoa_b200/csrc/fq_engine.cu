@@ -202,13 +202,8 @@ static int passes_for(int N, int lrows) {
 }
 
 // Row bits of the strided passes: the widest rows (best DRAM locality) that
-// still give the fewest passes.  FQ_LROWS overrides (1..8) for tuning.
+// still give the fewest passes.
 static int choose_lrows(int N) {
-    const char* e = getenv("FQ_LROWS");
-    if (e) {
-        const int v = atoi(e);
-        if (v >= 1 && v <= 8) return v;
-    }
     int best = 4;
     for (int lr = 4; lr >= 1; lr--)
         if (passes_for(N, lr) < passes_for(N, best)) best = lr;

@@ -1,5 +1,5 @@
-// fq_launch.cuh -- host-side launch of the tile passes (k_pass, k_pass_tma,
-// k_pass_tma2): schedule selection, TMA tensor maps, profiling brackets.
+// fq_launch.cuh -- host-side launch of the tile passes (k_pass, k_pass_tma):
+// schedule selection, TMA tensor maps, profiling brackets.
 // The kernel variants are instantiated in a few translation units
 // (fq_disp_*.cu) so they compile in parallel; fq_engine.cu calls the
 // dispatch_* entry points declared at the end.
@@ -13,7 +13,6 @@
 #include "fq_ctx.h"
 #include "fq_pass.cuh"
 #include "fq_pass_tma.cuh"
-#include "fq_pass_ws.cuh"
 
 namespace fq {
 
@@ -67,38 +66,10 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     return fn;
 }
 
-// Which passes run as TMA pipelines (FQ_TMA overrides; measured on B200 at
-// N=30, see the profiles):
-//   0  none (every pass uses per-thread loads, k_pass)
-//   1  passes without a cost phase use the one-group TMA pass (default:
-//      strided passes are fastest there, the phase pass with k_pass)
-//   2  every read-write pass uses the two-group TMA pass (<C> passes the
-//      one-group one)
-//   3  every read-write pass uses the one-group TMA pass
-inline int tma_mode() {
-    static int m = -1;
-    if (m < 0) {
-        const char* e = getenv("FQ_TMA");
-        m = e ? std::max(0, std::min(3, atoi(e))) : 1;
-    }
-    return m;
-}
-inline bool tma_for(int ph) {
-    const int m = tma_mode();
-    return m >= 2 || (m == 1 && ph == PH_NONE);
-}
-
-// FQ_WS=1 runs strided RX passes (no phase, no <C>) as the warp-specialised
-// pipeline with TMA stores (k_pass_ws) instead of k_pass_tma.  Off by
-// default: on B200 at N=30 it measured 4552 GB/s against 4828 GB/s.
-inline bool ws_enabled() {
-    static int m = -1;
-    if (m < 0) {
-        const char* e = getenv("FQ_WS");
-        m = e ? (atoi(e) != 0) : 0;
-    }
-    return m != 0;
-}
+// Read-write passes without a cost phase (the strided RX passes) run as
+// the TMA pipeline k_pass_tma; passes with a phase use k_pass, whose two
+// CTAs per SM measured faster for them on B200 at N=30.
+inline bool tma_for(int ph) { return ph == PH_NONE; }
 
 // The state as a tensor of float64 whose innermost dimension is one 128-byte
 // row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
@@ -150,33 +121,10 @@ template <typename WT, int PH, int GM, int EX, int SC>
 inline int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, TmaGeom G) {
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
     const int tok = prof_begin(ctx);
-    bool launched = false;
-    if constexpr (PH == PH_NONE && EX == EX_NONE && GM != GM_NONE) {
-        if (ws_enabled()) {
-            auto fn = k_pass_ws<GM, SC>;
-            FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)ws_pass_smem_bytes()));
-            fn<<<(unsigned)grid, kWsThreads, ws_pass_smem_bytes(), ctx->stream>>>(A, map, G);
-            launched = true;
-        }
-    }
-    if constexpr (EX == EX_NONE) {
-        if (!launched && tma_mode() == 2) {
-            auto fn = k_pass_tma2<WT, PH, GM, EX, SC>;
-            FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)tma2_pass_smem_bytes<WT>(kMaxQubits)));
-            fn<<<(unsigned)grid, 2 * kPassThreads, tma2_pass_smem_bytes<WT>(A.N),
-                 ctx->stream>>>(A, map, G);
-            launched = true;
-        }
-    }
-    if (!launched) {
-        auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
-        FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
-        fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map,
-                                                                                        G);
-    }
+    auto fn = k_pass_tma<WT, PH, GM, EX, SC>;
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
+    fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map, G);
     FQ_CUDA(cudaGetLastError());
     prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
     ctx->launches++;

@@ -30,7 +30,6 @@ constexpr unsigned kTileBytes = kTile * sizeof(double2);  // 64 KB
 // the thread for ~4 us on B200 (2^16 polls measured 0.26 s), so 2^18 polls
 // give up after about a second; a landing copy ends the wait at once.
 constexpr long long kWaitSpins = 1ll << 18;
-constexpr long long kIssueSpins = 1ll << 22;  // polls of 32 ns sleeps (two-group stage guard)
 
 // Box geometry of a pass (host-chosen, see make_pass_tmap):
 //   TG_CONTIG  l = 12: rank 3, box {16 doubles, 256 rows, 2}
@@ -319,319 +318,6 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         if (tid == 0) {
             double sum = 0;
             for (int w = 0; w < kPassThreads / 32; w++) sum += red[w];
-            A.partial[blockIdx.x] = sum;
-        }
-    }
-}
-
-
-// Shared-memory bytes of the two-group TMA pass.
-template <typename WT>
-__host__ __device__ inline size_t tma2_pass_smem_bytes(int N) {
-    return 1024 + (size_t)kStages * kTileBytes + 128 + sizeof(double) * 16 + sizeof(i64) * 32 +
-           sizeof(int) * 24 + sizeof(WT) * (N * N + 2 * 32 + 16 + 24 + 16) + 16 +
-           (sizeof(WT) == sizeof(int) ? phase_smem_bytes() : 0);
-}
-
-// The TMA pass with two 256-thread consumer groups per CTA (512 threads, one
-// CTA per SM).  Group g computes this CTA's tiles j = g, g+2, ... from the
-// shared 3-stage ring and synchronises on its own named barrier, so one
-// group's barrier waits and shared-memory round trips overlap the other's
-// arithmetic.  When a group has made its last shared-memory read of tile j,
-// its thread 0 refills that stage with tile j+3 (which the other group
-// computes).  A group may reach tile j before the other group has released
-// tile j-3 from the same stage; it then waits for the stage's issued-tile
-// index to reach j before its mbarrier parity wait (the parity of a stage
-// still in tile j-3's phase would otherwise read as "complete").
-template <typename WT, int PH, int GM, int EX, int SC>
-__global__ void __launch_bounds__(2 * kPassThreads, 1)
-    k_pass_tma2(const PassArgs A, const __grid_constant__ CUtensorMap tmap, const TmaGeom G) {
-    extern __shared__ unsigned char smraw[];
-    unsigned char* sm = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~(uintptr_t)1023);
-    double2* stage = reinterpret_cast<double2*>(sm);
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + kStages * kTileBytes);
-    int* s_abort = reinterpret_cast<int*>(full + kStages);         // [2]
-    long long* issued = reinterpret_cast<long long*>(full + 8);    // [kStages] last tile issued
-    double* red = reinterpret_cast<double*>(full + 16);            // [16]
-    i64* offtab = reinterpret_cast<i64*>(red + 16);
-    int* fpos = reinterpret_cast<int*>(offtab + 32);
-    WT* sw = reinterpret_cast<WT*>(fpos + 24);
-    WT* ke_all = sw + A.N * A.N;                                     // [2][32]
-    WT* creg = ke_all + 64;
-    WT* Dm = creg + 16;
-    WT* Ru = Dm + 24;
-    double2* smtab = reinterpret_cast<double2*>(
-        (reinterpret_cast<uintptr_t>(Ru + 16) + 15) & ~(uintptr_t)15);
-    constexpr bool CUT = (PH != PH_NONE) || (EX == EX_ENERGY);
-    const int N = A.N, l = A.l, a = A.a;
-    const int nF = N - kTileBits;
-    const int nmid = a - l;
-    const int g = threadIdx.x >> 8, tid = threadIdx.x & 255;
-    const int lane = tid & 31, warp = tid >> 5;
-    WT* ke = ke_all + 32 * g;
-    const i64 my_tiles =
-        blockIdx.x < A.ntiles ? (A.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-
-    auto issue = [&](i64 j) {
-        const i64 T = blockIdx.x + j * (i64)gridDim.x;
-        const int s = (int)(j % kStages);
-        void* dst = stage + (size_t)s * kTile;
-        issued[s] = j;
-        mbar_expect_tx(&full[s], kTileBytes);
-        if (G.kind == TG_CONTIG) {
-            tma_load_3d(dst, &tmap, &full[s], 0, 0, (int)(2 * T));
-        } else if (G.kind == TG_ROWS) {
-            tma_load_5d(dst, &tmap, &full[s], 0, 0, (int)(T & ((1ll << nmid) - 1)), 0,
-                        (int)(T >> nmid));
-        } else {
-            tma_load_5d(dst, &tmap, &full[s], 0, (int)(T & ((1ll << nmid) - 1)), 0, 0,
-                        (int)(T >> nmid));
-        }
-    };
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) {
-            mbar_init(&full[s], 1);
-            issued[s] = -1;
-        }
-        s_abort[0] = s_abort[1] = 0;
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    if (threadIdx.x < 2 * kRegs) {
-        const int r = threadIdx.x & 15, lo = threadIdx.x < kRegs ? 8 : 4;
-        i64 o = 0;
-        for (int k = 0; k < 4; k++)
-            if ((r >> k) & 1) o += 1ll << tile_phys(lo + k, l, a);
-        offtab[threadIdx.x] = o;
-    }
-    if (CUT) {
-        const WT* gw = reinterpret_cast<const WT*>(A.w);
-        for (int i = threadIdx.x; i < N * N; i += 2 * kPassThreads) sw[i] = gw[i];
-        if (threadIdx.x < nF)
-            fpos[threadIdx.x] = threadIdx.x < nmid ? l + threadIdx.x
-                                                   : a + (kTileBits - l) + (threadIdx.x - nmid);
-    }
-    if (PH != PH_NONE && sizeof(WT) == sizeof(int))
-        load_phase_tables(A, smtab, threadIdx.x, 2 * kPassThreads);
-    __syncthreads();
-    if (threadIdx.x == 0)
-        for (i64 j = 0; j < kStages && j < my_tiles; j++) issue(j);
-    if (CUT) {
-        if (threadIdx.x < nF) {
-            const int m = fpos[threadIdx.x];
-            WT d = 0;
-            for (int u = 0; u < kTileBits; u++) d += sw[m * N + tile_phys(u, l, a)];
-            Dm[threadIdx.x] = d;
-        } else if (threadIdx.x >= 32 && threadIdx.x < 32 + kTileBits) {
-            const int u = tile_phys(threadIdx.x - 32, l, a);
-            WT r = 0;
-            for (int i = 0; i < nF; i++) r += sw[u * N + fpos[i]];
-            Ru[threadIdx.x - 32] = r;
-        } else if (threadIdx.x >= 64 && threadIdx.x < 80) {
-            const int r = threadIdx.x - 64;
-            WT c = 0;
-            for (int k = 0; k < 4; k++)
-                for (int k2 = k + 1; k2 < 4; k2++)
-                    if (((r >> k) ^ (r >> k2)) & 1)
-                        c += sw[tile_phys(8 + k, l, a) * N + tile_phys(8 + k2, l, a)];
-            creg[r] = c;
-        }
-    }
-    __syncthreads();
-    WT athr = 0, f0 = 0, f1 = 0, f2 = 0, f3 = 0;
-    if (CUT) {
-        for (int j = 0; j < 8; j++) {
-            const int pj = tile_phys(j, l, a);
-            const int tj = (tid >> j) & 1;
-            for (int j2 = j + 1; j2 < 8; j2++)
-                if (tj ^ ((tid >> j2) & 1)) athr += sw[pj * N + tile_phys(j2, l, a)];
-            const WT w0 = sw[pj * N + tile_phys(8, l, a)], w1 = sw[pj * N + tile_phys(9, l, a)];
-            const WT w2 = sw[pj * N + tile_phys(10, l, a)], w3 = sw[pj * N + tile_phys(11, l, a)];
-            if (tj) {
-                athr += w0 + w1 + w2 + w3;
-                f0 -= w0;
-                f1 -= w1;
-                f2 -= w2;
-                f3 -= w3;
-            } else {
-                f0 += w0;
-                f1 += w1;
-                f2 += w2;
-                f3 += w3;
-            }
-        }
-    }
-    i64 thr_off = 0, thr_off1 = 0;
-    for (int j = 0; j < 8; j++) thr_off |= (i64)((tid >> j) & 1) << tile_phys(j, l, a);
-    {
-        const int t1 = lay_index<1>(tid, 0);
-        for (int j = 0; j < kTileBits; j++)
-            if ((t1 >> j) & 1) thr_off1 |= 1ll << tile_phys(j, l, a);
-    }
-    const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
-    const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
-    double acc = 0, comp = 0;
-
-    for (i64 j = g; j < my_tiles; j += 2) {
-        const i64 T = blockIdx.x + j * (i64)gridDim.x;
-        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
-        const int s = (int)(j % kStages);
-        double2* buf = stage + (size_t)s * kTile;
-        if (CUT && warp == 0) {
-            WT h = 0;
-            if (lane < nF) {
-                const int m = fpos[lane];
-                const int zm = (int)((base >> m) & 1);
-                if (zm) h += Dm[lane];
-                for (int i = lane + 1; i < nF; i++)
-                    if (zm ^ (int)((base >> fpos[i]) & 1)) h += sw[m * N + fpos[i]];
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-            if (lane < kTileBits) {
-                const int u = tile_phys(lane, l, a);
-                WT e = Ru[lane];
-                for (int i = 0; i < nF; i++)
-                    if ((base >> fpos[i]) & 1) e -= 2 * sw[u * N + fpos[i]];
-                ke[1 + lane] = e;
-            }
-            if (lane == 0) ke[0] = h;
-        }
-        // Tile j enters stage s only after the other group has released tile
-        // j-3 from it.  Until then the stage's mbarrier may still be in tile
-        // j-3's phase, whose parity differs from tile j's, so a parity wait
-        // would return at once: wait for the issue first (bounded).
-        bool ok = false;
-        for (long long i = 0; i < kIssueSpins; i++) {
-            if (*(volatile long long*)&issued[s] == j) {
-                ok = true;
-                break;
-            }
-            __nanosleep(32);
-        }
-        if (!ok || !mbar_wait_bounded(&full[s], (unsigned)((j / kStages) & 1))) {
-            s_abort[g] = 1;
-            if (A.err) atomicExch(A.err, 1);
-        }
-        group_sync(g);  // tile landed (or abort), ke visible
-        if (s_abort[g]) break;
-
-        double2 v[kRegs];
-#pragma unroll
-        for (int r = 0; r < kRegs; r++) v[r] = buf[tslot(lay_index<0>(tid, r))];
-        WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
-        if (CUT) {
-            cbase = ke[0] + athr;
-#pragma unroll
-            for (int jj = 0; jj < 8; jj++)
-                if ((tid >> jj) & 1) cbase += ke[1 + jj];
-            g0 = f0 + ke[9];
-            g1 = f1 + ke[10];
-            g2 = f2 + ke[11];
-            g3 = f3 + ke[12];
-        }
-        // Refill the stage as soon as the group's last read of it is done.
-        auto release = [&]() {
-            group_sync(g);
-            if (tid == 0 && j + kStages < my_tiles) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                issue(j + kStages);
-            }
-        };
-        constexpr bool XCH = (GM != GM_NONE && SC != SC_L0);
-        if (!XCH) release();
-        if (PH != PH_NONE) {
-#pragma unroll
-            for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
-                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
-                double2 ph;
-                if (sizeof(WT) == sizeof(int)) {
-                    ph = int_phase(A, smtab, (int)cr);
-                } else {
-                    const double S = 2.0 * (double)cr - A.W;
-                    double sn, cs;
-                    sincos(S * A.gamma / 2, &sn, &cs);
-                    ph.x = cs;
-                    ph.y = sn;
-                }
-                if (PH == PH_INIT) {
-                    v[r].x = ph.x * A.scale;
-                    v[r].y = ph.y * A.scale;
-                } else {
-                    if (sizeof(WT) != sizeof(int)) {
-                        ph.x *= A.scale;
-                        ph.y *= A.scale;
-                    }
-                    const double2 in = v[r];
-                    v[r].x = in.x * ph.x - in.y * ph.y;
-                    v[r].y = in.x * ph.y + in.y * ph.x;
-                }
-            }
-        }
-        constexpr int LAY = (XCH && EX == EX_NONE) ? 1 : 0;
-        if (GM != GM_NONE) {
-            rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
-            if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
-            if (SC == SC_L021) {
-                exchange_g<0, 2>(v, buf, tid, g);
-                rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
-                exchange_g<2, 1>(v, buf, tid, g);
-            } else if (SC == SC_L01) {
-                exchange_g<0, 1>(v, buf, tid, g);
-            }
-            if (SC != SC_L0) {
-                if (LAY == 0) {
-                    rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                    exchange_g<1, 0>(v, buf, tid, g);
-                    release();
-                } else {
-                    release();
-                    rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                }
-            }
-        }
-        if (EX == EX_ENERGY) {
-            double ts = 0;
-#pragma unroll
-            for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
-                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
-                ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
-            }
-            const double y = ts - comp;
-            const double t2 = acc + y;
-            comp = (t2 - acc) - y;
-            acc = t2;
-        }
-        if (LAY == 0) {
-            double2* const p = A.sv + base + thr_off;
-#pragma unroll
-            for (int r = 0; r < kRegs; r++) __stcs(p + offtab[r], v[r]);
-        } else {
-            double2* const p1 = A.sv + base + thr_off1;
-#pragma unroll
-            for (int r = 0; r < kRegs; r++) __stcs(p1 + offtab[kRegs + r], v[r]);
-        }
-    }
-    __syncthreads();
-    if (s_abort[0] || s_abort[1]) {
-        // Drain copies still in flight into the stages (bounded), then leave.
-        if (threadIdx.x == 0)
-            for (int s = 0; s < kStages; s++)
-                if (issued[s] >= 0)
-                    mbar_wait_bounded(&full[s], (unsigned)((issued[s] / kStages) & 1));
-        return;
-    }
-    if (EX == EX_ENERGY) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) red[g * 8 + warp] = acc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double sum = 0;
-            for (int w = 0; w < 16; w++) sum += red[w];
             A.partial[blockIdx.x] = sum;
         }
     }

@@ -348,23 +348,53 @@ void orc_energy_grad(int N, int P, const double* graph_upper, const double* gamm
     free(lam);
 }
 
-void orc_layer_sample(double* sv, int N, int s, const double* graph1d, double gamma,
-                      double beta, double* t_cost, double* t_rx) {
-    const i64 n = 1ll << s;
-    const double amp = orc_init_amp(N);
-    double t0 = omp_get_wtime();
+void orc_state_fill(double* sv, int N, double re, double im) {
+    const i64 n = 1ll << N;
 #pragma omp parallel for schedule(static)
-    for (i64 b = 0; b < n; b++) {
+    for (i64 z = 0; z < n; z++) {
+        sv[2 * z] = re;
+        sv[2 * z + 1] = im;
+    }
+}
+
+void orc_layer_chunk(double* sv, int N, const double* graph1d, double gamma, double beta,
+                     int first_layer, int chunk, int nchunks, double* t_cost, double* t_rx) {
+    const i64 per = (1ll << N) / nchunks, pper = (1ll << (N - 1)) / nchunks;
+    const double amp = orc_init_amp(N);
+    const i64 a0 = (i64)chunk * per, p0 = (i64)chunk * pper;
+    double t0 = omp_get_wtime();
+    /* rzz.cu:121-156 on amplitudes [a0, a0 + per) */
+#pragma omp parallel for schedule(static)
+    for (i64 b = a0; b < a0 + per; b++) {
         double sum = pair_sum((u64)b, N, graph1d);
         double sn, cs;
         sincos(sum * gamma / 2, &sn, &cs);
-        sv[2 * b] = cs * amp;
-        sv[2 * b + 1] = sn * amp;
+        if (first_layer) {
+            sv[2 * b] = cs * amp;
+            sv[2 * b + 1] = sn * amp;
+        } else {
+            double re = sv[2 * b], im = sv[2 * b + 1];
+            sv[2 * b] = re * cs - im * sn;
+            sv[2 * b + 1] = re * sn + im * cs;
+        }
     }
     double t1 = omp_get_wtime();
-    int targets[64];
-    for (int q = 0; q < s; q++) targets[q] = q;
-    orc_multi_rotate_x(sv, s, targets, s, beta);
+    /* rx.cu:32-53 for every qubit on pairs [p0, p0 + pper) */
+    double s, c;
+    sincos(beta / 2, &s, &c);
+    for (int t = 0; t < N; t++) {
+#pragma omp parallel for schedule(static)
+        for (i64 k = p0; k < p0 + pper; k++) {
+            u64 up = insert_zero((u64)k, t);
+            u64 lo = up + (1ull << t);
+            double q0r = sv[2 * up], q0i = sv[2 * up + 1];
+            double q1r = sv[2 * lo], q1i = sv[2 * lo + 1];
+            sv[2 * up] = q0r * c + q1i * s;
+            sv[2 * up + 1] = q0i * c - q1r * s;
+            sv[2 * lo] = q0i * s + q1r * c;
+            sv[2 * lo + 1] = -q0r * s + q1i * c;
+        }
+    }
     double t2 = omp_get_wtime();
     *t_cost = t1 - t0;
     *t_rx = t2 - t1;

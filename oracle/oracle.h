@@ -66,13 +66,17 @@ void orc_energy_grad(int N, int P, const double* graph_upper, const double* gamm
                      double* grad_beta);
 /* dst[y] = src[x] where y has bit perm[b] equal to bit b of x. */
 void orc_permute_qubits(const double* src, double* dst, int N, const int* perm);
-/* CPU-baseline sample of one QAOA layer of an N-qubit circuit: the cost
- * phase of rzz.cu:121-156 (pair loop over the full N-qubit graph) on the
- * first 2^s amplitudes, then RX (rx.cu:32-53) on qubits 0..s-1 of that
- * slice.  Returns the seconds each half took; a full layer is
- * t_cost * 2^(N-s) + t_rx * (N * 2^(N-1)) / (s * 2^(s-1)). */
-void orc_layer_sample(double* sv, int N, int s, const double* graph1d, double gamma,
-                      double beta, double* t_cost, double* t_rx);
+/* Every amplitude set to re + i*im (OpenMP first touch). */
+void orc_state_fill(double* sv, int N, double re, double im);
+/* CPU-baseline unit of work: chunk `chunk` of `nchunks` equal parts of one
+ * QAOA layer on a full 2^N state -- the cost phase of rzz.cu:121-156 (pair
+ * loop over the whole graph) on amplitudes [chunk, chunk+1) * 2^N/nchunks,
+ * then RX (rx.cu:32-53) for every qubit t on pairs [chunk, chunk+1) *
+ * 2^(N-1)/nchunks of t's pair enumeration.  The nchunks parts together do
+ * exactly one layer's amplitude and pair updates.  Returns each half's
+ * seconds. */
+void orc_layer_chunk(double* sv, int N, const double* graph1d, double gamma, double beta,
+                     int first_layer, int chunk, int nchunks, double* t_cost, double* t_rx);
 /* Threads OpenMP will use. */
 int orc_num_threads(void);
 

@@ -51,8 +51,9 @@ def lib():
                                       _dp, _dp, _dp]
         L.orc_permute_qubits.argtypes = [_dp, _dp, ctypes.c_int, _ip]
         L.orc_num_threads.restype = ctypes.c_int
-        L.orc_layer_sample.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double,
-                                       ctypes.c_double, _dp, _dp]
+        L.orc_state_fill.argtypes = [_dp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.orc_layer_chunk.argtypes = [_dp, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
         _lib = L
     return _lib
 
@@ -191,18 +192,41 @@ def to_logical(sv_phys, label_map):
     return permute_qubits(sv_phys, label_map)
 
 
-def layer_sample(graph, s, gamma, beta):
-    """Time one layer's work units on a 2^s-amplitude slice of the N-qubit
-    circuit; returns (t_cost, t_rx, estimated seconds for the full layer)."""
-    g = _f64(graph)
-    n = g.shape[0]
-    g1d = upper_tri_to_1d(g)
-    if len(g1d) == 0:
-        g1d = np.zeros(1)
-    sv = np.zeros(1 << s, dtype=np.complex128)
-    tc = np.zeros(1)
-    tr = np.zeros(1)
-    lib().orc_layer_sample(sv.view(np.float64).ctypes.data_as(_dp), n, s, _d(g1d), gamma,
-                           beta, _d(tc), _d(tr))
-    full = tc[0] * 2.0 ** (n - s) + tr[0] * (n * 2.0 ** (n - 1)) / (s * 2.0 ** (s - 1))
-    return float(tc[0]), float(tr[0]), full
+class CpuLayer:
+    """One QAOA layer of the reference algorithm on a full 2^N host state,
+    timed in equal parts (orc_layer_chunk): the CPU baseline of the bench.
+    The state is allocated and first-touched once (16 GiB at N = 30)."""
+
+    def __init__(self, graph, nchunks=32):
+        g = _f64(graph)
+        self.n = g.shape[0]
+        g1d = upper_tri_to_1d(g)
+        self.g1d = g1d if len(g1d) else np.zeros(1)
+        self.nchunks = nchunks
+        self.sv = np.empty(1 << self.n, dtype=np.complex128)
+        lib().orc_state_fill(self._p(), self.n, 2.0 ** (-self.n / 2), 0.0)
+
+    def _p(self):
+        return self.sv.view(np.float64).ctypes.data_as(_dp)
+
+    def chunk(self, k, gamma, beta):
+        """Part k of a layer (not the first: the cost phase reads and
+        multiplies); returns its seconds."""
+        tc, tr = np.zeros(1), np.zeros(1)
+        lib().orc_layer_chunk(self._p(), self.n, _d(self.g1d), gamma, beta, 0,
+                              k % self.nchunks, self.nchunks, _d(tc), _d(tr))
+        return float(tc[0] + tr[0])
+
+    def full_layer(self, gamma, beta):
+        """One whole layer in the reference's order (the read-multiply cost
+        phase of rzz.cu:152-154 on every amplitude, then RX on qubits 0..N-1,
+        rx.cu:32-53); returns its seconds."""
+        import time
+        t0 = time.perf_counter()
+        lib().orc_cost_phase(self._p(), self.n, gamma, _d(self.g1d), 0, init_amp(self.n))
+        tg = np.arange(self.n, dtype=np.int32)
+        lib().orc_multi_rotate_x(self._p(), self.n, _i(tg), self.n, beta)
+        return time.perf_counter() - t0
+
+    def free(self):
+        self.sv = None

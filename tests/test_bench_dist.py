@@ -55,15 +55,21 @@ def _json_lines(text):
 
 
 def test_reference_arm_line():
-    r = subprocess.run([sys.executable, BENCH, "--impl", "reference", "--steps", "1",
-                        "--warmup", "1", "--cpu-slice-bits", "16"],
+    """The reference arm on a 2^20-amplitude state (the default is the
+    benchmark's N=30, 16 GiB of host memory): its line carries the GPU arm's
+    workload config, the parts' timing and the whole-layer check."""
+    r = subprocess.run([sys.executable, BENCH, "--impl", "reference", "--steps", "2",
+                        "--warmup", "1", "--n", "20", "--no-ref-gpu"],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     (line,) = _json_lines(r.stdout)
     assert line["impl"] == "reference" and line["unit"] == "layers/s"
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"]["h2d_bytes_per_step"] == 0
-    assert line["config"]["N"] == 30
+    assert line["config"]["N"] == 20 and "engine" not in line["config"]
+    assert line["cpu_baseline"]["full_layer_s"] > 0 and line["cpu_baseline"]["scale_check"] > 0
+    assert line["layers_per_step"] == 1 / 32
+    assert abs(line["value"] * line["ms_per_step"] / 1000 - 1 / 32) < 1e-9
 
 
 def test_reference_arm_under_torchrun_prints_once():
@@ -71,7 +77,7 @@ def test_reference_arm_under_torchrun_prints_once():
     r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
                         "--nproc-per-node", "2", "--master-addr", "127.0.0.1", "--master-port",
                         str(port), BENCH, "--impl", "reference", "--gpus", "2", "--steps", "1",
-                        "--warmup", "1", "--cpu-slice-bits", "16"],
+                        "--warmup", "1", "--qubits", "18", "--no-ref-gpu"],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)

@@ -441,3 +441,32 @@ def test_refapi_unweighted_bitmask_path(fq, oracle, tmp_path):
     got = np.empty_like(phys)
     got[x] = phys
     assert_state_close(got, want, what="C++ API, unweighted graph")
+
+
+def test_refapi_state_setup_and_copies(oracle, tmp_path):
+    """stateCpyHostToDevice, stateInitDeviceState and prepare
+    (src/state.cpp:162-219,328-336) through a program written only against
+    the reference-style C++ API (tests/refapi_state_io.cpp): an uploaded host
+    state is what the next kernel (multiRotateX on the first C qubits) acts
+    on, checked against the oracle; the device state resets to |0...0>; the
+    chunk size is recorded and C < 1 is refused."""
+    import shutil
+    cxx = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    exe = tmp_path / "refapi_state_io"
+    here = os.path.dirname(os.path.abspath(__file__))
+    inc = os.path.join(os.path.dirname(here), "include")
+    r = subprocess.run([cxx, "-std=c++17", "-I", inc, os.path.join(here, "refapi_state_io.cpp"),
+                        "-L", PKG, "-lforqaoa", "-Xlinker", "-rpath=" + PKG, "-o", str(exe)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    N, C, angle = 15, 6, 0.83
+    pre = tmp_path / "st"
+    r = subprocess.run([str(exe), str(N), str(C), str(angle), str(pre)], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split("\n")[:4] == ["createState |0> ok", "stateCpyHostToDevice + multiRotateX ok",
+                                        "stateInitDeviceState ok", "prepare ok"]
+    sv_in = np.fromfile(str(pre) + ".in", dtype=np.complex128)
+    got = np.fromfile(str(pre) + ".out", dtype=np.complex128)
+    want = oracle.multi_rotate_x(sv_in.copy(), N, list(range(C)), angle)
+    assert_state_close(got, want, what="host state uploaded, then RX on qubits 0..C-1")
