@@ -81,8 +81,10 @@ def parse_args(argv=None):
                     help="reference arm: skip timing the reference's own CUDA build")
     ap.add_argument("--no-cpu-full", action="store_true",
                     help="skip the whole-layer CPU measurement (parts only)")
-    ap.add_argument("--serve-requests", type=int, default=1000,
+    ap.add_argument("--serve-requests", type=int, default=10000,
                     help="requests of the served-stream leg (0: skip it)")
+    ap.add_argument("--serve-sustained-requests", type=int, default=1200,
+                    help="requests of the served leg's sustainable-rate latency run")
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--no-grad", action="store_true", help="skip the adjoint-gradient leg")
     return ap.parse_args(argv)
@@ -533,33 +535,89 @@ def gradient_leg(ctx, peak, n=26, P=10, reps=5):
     return out
 
 
-def serving_leg(args):
-    """A scaled sample of the served stream (sessions of 20 energy+gradient
-    steps, N ~ U{10..28}, p ~ U{1..8}, G(N,0.5) integer weights, Poisson
-    session arrivals, 150 GB budget): evals/s and p50/p99 latency through the
-    server, against the same evaluations as sequential plain calls."""
+def eval_bytes(ctx, n, P, cache):
+    """Algorithmic HBM bytes of one energy+gradient evaluation (the library's
+    per-launch accounting, summed over one evaluation), cached per (n, P)."""
+    key = (n, P)
+    if key not in cache:
+        rng = np.random.default_rng(n * 100 + P)
+        W = np.triu(rng.integers(1, 11, size=(n, n)).astype(np.float64), 1)
+        ctx.profile_reset()
+        ctx.set_profiling(True)
+        ctx.energy_grad(n, W, rng.uniform(0, np.pi, P), rng.uniform(0, np.pi / 2, P))
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        cache[key] = sum(v[2] for v in prof.values())
+    return cache[key]
+
+
+def serving_ceiling(seq, peak_gbs, sms):
+    """Best speed-up over sequential calls this stream allows: every request
+    at least its HBM roofline time (algorithmic bytes / measured copy
+    bandwidth; requests share one HBM), a one-CTA request (N <= 12) at least
+    its sequential time spread over every SM.  ceiling = sum of sequential
+    times / sum of those bounds."""
     import forqaoa
+    cache = {}
+    t_seq = t_bound = 0.0
+    with forqaoa.Context(0) as ctx:
+        for r in seq:
+            t_seq += r["latency"]
+            if r["N"] <= 12:
+                t_bound += r["latency"] / sms
+            else:
+                t_bound += eval_bytes(ctx, r["N"], r["P"], cache) / (peak_gbs * 1e9)
+    return t_seq / t_bound, t_seq, t_bound
+
+
+def serving_leg(args):
+    """The served stream (config 5: sessions of 20 energy+gradient steps,
+    N ~ U{10..28}, p ~ U{1..8}, G(N,0.5) integer weights, Poisson session
+    arrivals, 150 GB budget), every request loop driven natively
+    (serve_replay): evals/s and p50/p99 latency through the server against
+    the same evaluations as sequential calls, the speed-up ceiling this
+    stream allows, latency at a sustainable arrival rate, and the stream per
+    size class (by_size) against sequential and plain calls."""
     import serve_stream as ss
+    peak, _ = hbm_peak()
     sessions, steps = ss.make_stream(args.serve_requests, seed=5)
-    ss.run_served(forqaoa, sessions[:2], 1, lanes=args.serve_lanes)  # warm-up
-    served, wall, stats = ss.run_served(forqaoa, sessions, steps, lanes=args.serve_lanes)
-    seq, wall_q = ss.run_sequential(forqaoa, sessions, steps)
-    plain, wall_p = ss.run_sequential(forqaoa, sessions, steps, reuse=False)
-    out = ss.summarize(served, wall, seq, wall_q, stats, plain, wall_p)
+    ss.run_native("served", sessions[:4], 2, lanes=args.serve_lanes)  # warm-up
+    served, wall, info = ss.run_native("served", sessions, steps, lanes=args.serve_lanes)
+    seq, wall_q, _ = ss.run_native("sequential", sessions, steps)
+    out = ss.summarize(served, wall, seq, wall_q, None)
+    out["server"] = info
+    ceil, t_seq, t_bound = serving_ceiling(seq, peak, 148)
+    out["ceiling_speedup_vs_sequential"] = ceil
+    out["ceiling_note"] = ("sum of sequential times %.1f s / sum of per-request bounds %.1f s "
+                           "(HBM roofline of each request's algorithmic bytes at %.0f GB/s; "
+                           "one-CTA requests: sequential time / 148 SMs)" % (t_seq, t_bound, peak))
     out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [10, 28], "p": [1, 8],
                      "graph": "G(N,0.5), integer weights 1..10", "seed": 5,
-                     "arrivals": "Poisson, mean gap 1 ms", "lanes": args.serve_lanes,
-                     "budget_gb": 150, "sample_of": "10,000-request stream"}
+                     "arrivals": "Poisson, mean gap 1 ms (arrivals outpace the device: "
+                                 "latency includes queueing)",
+                     "lanes": args.serve_lanes, "budget_gb": 150,
+                     "client": "serve_replay (native closed loop)"}
+    # Latency where the server keeps up: sessions arriving at 80% of the
+    # session rate just measured.
+    cap_sessions_per_s = out["evals_per_s"] / steps
+    gap_ms = 1000.0 / (0.8 * cap_sessions_per_s)
+    sus, _ = ss.make_stream(args.serve_sustained_requests, seed=6, mean_gap_ms=gap_ms)
+    sv, w, _ = ss.run_native("served", sus, steps, lanes=args.serve_lanes)
+    r = ss.summarize(sv, w)
+    out["sustained"] = {"requests": r["requests"], "arrival_gap_ms": gap_ms,
+                        "load": "80% of the session rate measured above",
+                        "evals_per_s": r["evals_per_s"], "latency_ms_p50": r["latency_ms_p50"],
+                        "latency_ms_p99": r["latency_ms_p99"], "queue_ms_p50": r["queue_ms_p50"]}
     # The same stream restricted to one size class at a time: the mixed
     # stream's time is dominated by N = 27..28 (HBM-bound one at a time),
     # these show what batching and overlap do where a request is not.
     out["by_size"] = {}
-    for lo, hi, n_req, lanes in ((10, 12, 2000, args.serve_lanes), (13, 20, 400, 8),
+    for lo, hi, n_req, lanes in ((10, 12, 2000, args.serve_lanes), (13, 20, 2000, 8),
                                  (21, 28, 200, args.serve_lanes)):
         sess, steps = ss.make_stream(n_req, seed=lo, n_min=lo, n_max=hi)
-        sv, w, st = ss.run_served(forqaoa, sess, steps, lanes=lanes)
-        sq, wq = ss.run_sequential(forqaoa, sess, steps)
-        pl, wp = ss.run_sequential(forqaoa, sess, steps, reuse=False)
+        sv, w, _ = ss.run_native("served", sess, steps, lanes=lanes)
+        sq, wq, _ = ss.run_native("sequential", sess, steps)
+        pl, wp, _ = ss.run_native("plain", sess, steps)
         r = ss.summarize(sv, w, sq, wq, None, pl, wp)
         out["by_size"][f"N {lo}..{hi}"] = {
             k: r[k] for k in ("requests", "evals_per_s", "latency_ms_p50", "latency_ms_p99",

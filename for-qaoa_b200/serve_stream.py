@@ -128,6 +128,52 @@ def run_sequential(fq, sessions, steps, device=0, reuse=True):
     return recs, wall
 
 
+REPLAY = os.path.join(HERE, "serve_replay")
+
+
+def write_stream(sessions, steps, path):
+    """The stream in serve_replay's input format."""
+    with open(path, "wb") as f:
+        f.write(np.array([len(sessions), steps], dtype=np.int32).tobytes())
+        for s in sessions:
+            f.write(np.array([s["id"], s["N"], s["P"]], dtype=np.int32).tobytes())
+            f.write(np.array([s["arrival"]], dtype=np.float64).tobytes())
+            f.write(np.ascontiguousarray(s["graph"], dtype=np.float64).tobytes())
+            f.write(np.asarray(s["gammas"], dtype=np.float64).tobytes())
+            f.write(np.asarray(s["betas"], dtype=np.float64).tobytes())
+
+
+def read_records(path):
+    raw = open(path, "rb").read()
+    recs, off = [], 0
+    while off < len(raw):
+        sid, step, n, P = np.frombuffer(raw, dtype=np.int32, count=4, offset=off)
+        off += 16
+        d = np.frombuffer(raw, dtype=np.float64, count=3 + 2 * P, offset=off)
+        off += 8 * (3 + 2 * P)
+        recs.append({"session": int(sid), "step": int(step), "N": int(n), "P": int(P),
+                     "energy": float(d[0]), "latency": float(d[1]), "queue": float(d[2]),
+                     "grad_gamma": d[3:3 + P].copy(), "grad_beta": d[3 + P:].copy()})
+    return recs
+
+
+def run_native(mode, sessions, steps, lanes=4, budget=150e9):
+    """The stream through serve_replay (no Python in the request loop):
+    mode 'served', 'sequential' or 'plain'; returns (records, wall_s, info)."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "stream.bin"), os.path.join(td, "out.bin")
+        write_stream(sessions, steps, fin)
+        r = subprocess.run([REPLAY, fin, mode, fout, str(lanes), str(budget / 1e9)],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("serve_replay %s failed: %s" % (mode, r.stderr[-1000:]))
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        recs = read_records(fout)
+    return recs, info["wall_s"], info
+
+
 def pct(xs, q):
     return float(np.percentile(np.asarray(xs), q)) * 1000.0 if len(xs) else None
 
@@ -188,15 +234,23 @@ def main(argv=None):
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--gap-ms", type=float, default=1.0, help="mean session inter-arrival")
     ap.add_argument("--no-sequential", action="store_true")
+    ap.add_argument("--python-client", action="store_true",
+                    help="drive the stream from this Python loop instead of serve_replay")
     a = ap.parse_args(argv)
-    import forqaoa as fq
     sessions, steps = make_stream(a.requests, a.seed, a.steps, a.n_min, a.n_max, a.p_max,
                                   a.gap_ms)
-    served, wall, stats = run_served(fq, sessions, steps, 0, a.lanes, a.budget_gb * 1e9)
     seq = wall_q = plain = wall_p = None
-    if not a.no_sequential:
-        seq, wall_q = run_sequential(fq, sessions, steps)
-        plain, wall_p = run_sequential(fq, sessions, steps, reuse=False)
+    if a.python_client:
+        import forqaoa as fq
+        served, wall, stats = run_served(fq, sessions, steps, 0, a.lanes, a.budget_gb * 1e9)
+        if not a.no_sequential:
+            seq, wall_q = run_sequential(fq, sessions, steps)
+            plain, wall_p = run_sequential(fq, sessions, steps, reuse=False)
+    else:
+        served, wall, stats = run_native("served", sessions, steps, a.lanes, a.budget_gb * 1e9)
+        if not a.no_sequential:
+            seq, wall_q, _ = run_native("sequential", sessions, steps)
+            plain, wall_p, _ = run_native("plain", sessions, steps)
     out = summarize(served, wall, seq, wall_q, stats, plain, wall_p)
     out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [a.n_min, a.n_max],
                      "p": [1, a.p_max], "graph": "G(N,0.5), integer weights 1..10",

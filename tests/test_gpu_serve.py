@@ -121,3 +121,25 @@ def test_bad_requests_are_refused(fq):
         W, g, b = make_request(rng, 16, 2)
         t = srv.submit(2, W, g, b)
         assert srv.wait([t])[t].status == 0
+
+
+def test_native_replay_served_equals_one_at_a_time():
+    """The stream driven natively (serve_replay, no Python in the request
+    loop): every served result is bit-identical to the same evaluation run
+    one at a time, with buffers reused per session and with a plain call per
+    evaluation; every session's steps come back in order."""
+    import serve_stream as ss
+    sessions, steps = ss.make_stream(240, seed=9, steps=6, n_min=4, n_max=19, p_max=6,
+                                     mean_gap_ms=0.2)
+    served, wall, info = ss.run_native("served", sessions, steps, lanes=3, budget=8e9)
+    seq, wall_q, _ = ss.run_native("sequential", sessions, steps)
+    plain, wall_p, _ = ss.run_native("plain", sessions, steps)
+    assert len(served) == len(seq) == len(plain) == len(sessions) * steps
+    assert info["batched_requests"] + info["lane_requests"] == len(served)
+    assert info["batched_requests"] > 0 and info["lane_requests"] > 0
+    assert ss.compare(served, seq) == 0
+    assert ss.compare(served, plain) == 0
+    last = {}
+    for r in served:
+        assert r["step"] == last.get(r["session"], -1) + 1
+        last[r["session"]] = r["step"]
