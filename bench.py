@@ -240,6 +240,18 @@ def is_headline(args):
     return args.n == 30 and args.p == 5
 
 
+# The kernels behind each pass kind of the engine at N=30 (tiles of 4096
+# amplitudes; strided tiles of 128-byte rows run paired, 512 threads).
+KIND_KERNELS = {
+    "init_pass": "fq::k_pass, PH_INIT (layer 0: launch-control init + phase + RX, write-only, "
+                 "strided tile, paired)",
+    "phase_pass": "fq::k_pass with GM2 (fused two-layer pass: RX, next layer's phase, RX; "
+                  "strided tiles, paired)",
+    "mixer_pass": "fq::k_pass, PH_NONE (RX only: the contiguous pass over qubits 0..11, and "
+                  "the circuit's last pass)",
+}
+
+
 def ncu_traffic_per_launch(kind, args):
     """DRAM bytes (read + write) per launch of a pass kind at N=30 from the
     committed ncu summary (profiles/pass_kernels_n30_p5.md), or None (other
@@ -439,34 +451,38 @@ def run_ours(args):
            "h2d_bytes_per_step": 4 * args.n * args.n, "d2h_bytes_per_step": 8,
            "ms_per_step": 1000.0 * e2e_s / args.steps, "energy_last": energy}
 
-    # ---- roofline.  Dominant kernel: the strided pass (k_pass_tma, two of
-    # the three sweeps of every layer); per_layer: every pass of the layer
-    # (the contiguous phase pass k_pass included).
+    # ---- roofline.  The engine's tile passes by kind: the layer-0 pass
+    # (launch-control init, write-only), the phase passes (fused two-layer
+    # passes) and the mixer passes (RX only).  The dominant kernel is the kind
+    # with the largest share of device time; per_layer covers every pass.
     peak, peak_src = hbm_peak()
     kern = {}
     tot_ms = tot_b = tot_n = 0
-    for kind in ("layer_pass", "strided_pass"):
+    for kind in ("init_pass", "phase_pass", "mixer_pass"):
         if kind in prof:
             kms, kn, kb = prof[kind]
-            kern[kind] = {"launches": kn, "ms_avg": kms / kn,
+            kern[kind] = {"launches": kn, "ms_avg": kms / kn, "ms_total": kms,
                           "alg_bytes_per_launch": kb / kn, "gbs": kb / (kms / 1000.0) / 1e9,
                           "frac": kb / (kms / 1000.0) / 1e9 / peak,
                           "traffic": ncu_traffic_per_launch(kind, args)}
             tot_ms += kms
             tot_b += kb
             tot_n += kn
-    dom = kern.get("strided_pass") or kern.get("layer_pass") or {}
+    dom_kind = max(kern, key=lambda k: kern[k]["ms_total"]) if kern else None
+    dom = kern.get(dom_kind, {})
     layer_gbs = tot_b / (tot_ms / 1000.0) / 1e9 if tot_ms else None
     roofline = {"bound": "hbm", "achieved": dom.get("gbs"), "peak": peak, "unit": "GB/s",
                 "frac": dom.get("frac"),
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)" if
                 peak_src == "measured" else "fallback 6.65 TB/s",
                 "traffic": dom.get("traffic"),
-                "kernel": "fq::k_pass_tma (strided tile pass, TMA pipeline)",
+                "kernel": KIND_KERNELS.get(dom_kind),
+                "kind": dom_kind,
                 "alg_bytes_per_launch": dom.get("alg_bytes_per_launch"),
                 "per_layer": {"gbs": layer_gbs, "frac": layer_gbs / peak if layer_gbs else None,
                               "launches": tot_n,
-                              "kernels": "k_pass (phase and fused passes) + k_pass_tma",
+                              "kernels": "every tile pass of the circuit (fq::k_pass, "
+                                         "fq::k_pass_tma)",
                               "sweeps_per_layer": tot_n / (args.steps * args.p),
                               "alg_bytes_per_layer": tot_b / (args.steps * args.p),
                               "share_of_step": (tot_ms / ms) if ms else None},

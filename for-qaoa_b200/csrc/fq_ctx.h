@@ -11,6 +11,7 @@ struct fq_ctx {
     bool own_stream = false;
     int num_sms = 0;
     int ctas_per_sm = 2;  // resident pass CTAs per SM (64 KB tile each)
+    int last_grid = 0;    // CTAs (and <C> partials) of the last tile pass launched
     // Device scratch, allocated once at creation.
     void* d_w = nullptr;          // N*N weights (int32 or float64)
     double2* d_ptab = nullptr;    // integer phase table

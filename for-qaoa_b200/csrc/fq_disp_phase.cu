@@ -1,21 +1,26 @@
-// fq_disp_phase.cu -- passes with a cost phase: the layer pass of the fused
-// engine (phase + RX on tile bits 0..11, schedule L0 -> L2 -> L1) and the
+// fq_disp_phase.cu -- passes with a cost phase: the first pass of a layer
+// (phase + RX on the pass's tile qubits, any tile geometry) and the
 // reference-path cost layer alone (fq_cost_phase).
 #include "fq_launch.cuh"
 
 namespace fq {
 
+template <typename WT, int PH, int GM, int SC>
+static int phase_launch_sc(fq_ctx* ctx, const PassArgs& A) {
+    return launch_ldg<WT, PH, GM, EX_NONE, true, SC>(ctx, A);
+}
+
 template <typename WT, int PH, int GM>
 static int phase_launch(fq_ctx* ctx, const PassArgs& A) {
-    constexpr int SC = GM == GM_NONE ? SC_L0 : SC_L021;
-    FQ_CHECK(GM == GM_NONE || schedule_for(A.tmask) == SC_L021, FQ_ERR_INVALID,
-             "phase pass with gates needs two or more targets among tile bits 0..3");
-    if (PH == PH_MUL && tma_for(PH)) {
-        alignas(64) CUtensorMap map;
-        TmaGeom G;
-        if (make_pass_tmap(A, &map, &G)) return launch_tma<WT, PH, GM, EX_NONE, SC>(ctx, A, map, G);
+    if constexpr (GM == GM_NONE) {
+        return phase_launch_sc<WT, PH, GM, SC_L0>(ctx, A);
+    } else {
+        switch (schedule_for(A.tmask)) {
+            case SC_L021: return phase_launch_sc<WT, PH, GM, SC_L021>(ctx, A);
+            case SC_L01: return phase_launch_sc<WT, PH, GM, SC_L01>(ctx, A);
+            default: return phase_launch_sc<WT, PH, GM, SC_L0>(ctx, A);
+        }
     }
-    return launch_ldg<WT, PH, GM, EX_NONE, true, SC>(ctx, A);
 }
 
 template <typename WT>

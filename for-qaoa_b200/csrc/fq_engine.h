@@ -17,8 +17,9 @@ struct PassPlan {
     unsigned tmask;
 };
 
-// Passes of one layer for N >= 12: the contiguous tile (phase + qubits
-// 0..11) first, then strided tiles over the remaining qubits.
+// Passes of one layer for N >= 12: the contiguous tile over qubits 0..11
+// and strided tiles over the remaining qubits (the first strided one leads
+// when there are three or more passes); the first pass carries the phase.
 std::vector<PassPlan> plan_layer(int N);
 // Reduced RX for angle beta: gate mode, t or u, and the factor f.
 void gate_params(double beta, int& gm, double& g, double& f);

@@ -23,7 +23,8 @@ inline int pass_kind() {
     if (EX == EX_DIAG) return FQ_KIND_EXPECT;
     if (GM == GM_FULL) return FQ_KIND_RX;
     if (GM == GM_NONE) return FQ_KIND_COST;
-    return PH != PH_NONE ? FQ_KIND_LAYER_PASS : FQ_KIND_STRIDED_PASS;
+    if (PH == PH_INIT) return FQ_KIND_INIT_PASS;
+    return PH != PH_NONE ? FQ_KIND_PHASE_PASS : FQ_KIND_MIXER_PASS;
 }
 
 template <int PH, int EX, bool ST>
@@ -34,19 +35,34 @@ inline double pass_bytes(int N) {
                 (EX == EX_COSTATE ? 16.0 : 0.0));
 }
 
-template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE>
-inline int launch_ldg(fq_ctx* ctx, const PassArgs& A) {
-    auto fn = k_pass<WT, PH, GM, EX, ST, SC, GM2>;
-    const size_t smem = pass_smem_bytes<WT>(A.N);
-    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)pass_smem_bytes<WT>(kMaxQubits)));
-    const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->ctas_per_sm * ctx->num_sms);
+// Strided tiles with 128-byte rows run as paired CTAs (k_pass with PAIR:
+// the two tiles that differ in physical bit 3 at once, so DRAM sees 256-byte
+// rows).  Measured on B200 at N=30, p=5 (A/B in one call): 59.8-60.1
+// layers/s with every such pass paired, 59.5-59.7 with the strided RX pass
+// on the TMA pipeline instead.
+inline bool pair_ok(const PassArgs& A) { return A.l == 3 && A.a > A.l && A.ntiles >= 2; }
+
+template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
+          bool PAIR = false>
+inline int launch_ldg_as(fq_ctx* ctx, const PassArgs& A) {
+    auto fn = k_pass<WT, PH, GM, EX, ST, SC, GM2, PAIR>;
+    const size_t smem = pass_smem_bytes<WT>(A.N, PAIR);
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const i64 units = PAIR ? A.ntiles / 2 : A.ntiles;
+    const i64 grid = std::min<i64>(units, (i64)(PAIR ? 1 : ctx->ctas_per_sm) * ctx->num_sms);
     const int tok = prof_begin(ctx);
-    fn<<<(unsigned)grid, kPassThreads, smem, ctx->stream>>>(A);
+    fn<<<(unsigned)grid, PAIR ? 2 * kPassThreads : kPassThreads, smem, ctx->stream>>>(A);
     FQ_CUDA(cudaGetLastError());
+    ctx->last_grid = (int)grid;
     prof_end(ctx, tok, pass_kind<PH, GM, EX, ST>(), pass_bytes<PH, EX, ST>(A.N));
     ctx->launches++;
     return FQ_OK;
+}
+
+template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE>
+inline int launch_ldg(fq_ctx* ctx, const PassArgs& A) {
+    if (pair_ok(A)) return launch_ldg_as<WT, PH, GM, EX, ST, SC, GM2, true>(ctx, A);
+    return launch_ldg_as<WT, PH, GM, EX, ST, SC, GM2, false>(ctx, A);
 }
 
 inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
@@ -66,10 +82,15 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     return fn;
 }
 
-// Read-write passes without a cost phase (the strided RX passes) run as
-// the TMA pipeline k_pass_tma; passes with a phase use k_pass, whose two
-// CTAs per SM measured faster for them on B200 at N=30.
-inline bool tma_for(int ph) { return ph == PH_NONE; }
+// The TMA pipeline k_pass_tma runs the read-write RX passes (no cost phase)
+// over strided tiles with rows of 16 or more amplitudes.  Contiguous tiles
+// and tiles with 128-byte rows (paired) run on k_pass, whose per-thread
+// loads from two CTAs per SM measured faster there on B200 at N=30 (the
+// contiguous RX pass: 6.0 ms against 6.9 ms on the TMA pipeline); passes
+// with a phase always do.
+inline bool tma_for(int ph, const PassArgs& A) {
+    return ph == PH_NONE && A.l >= 4 && A.l < kTileBits;
+}
 
 // The state as a tensor of float64 whose innermost dimension is one 128-byte
 // row of 8 amplitudes; the box is one tile (4096 amplitudes) in tile order.
@@ -126,20 +147,20 @@ inline int launch_tma(fq_ctx* ctx, const PassArgs& A, const CUtensorMap& map, Tm
                                  (int)tma_pass_smem_bytes<WT>(kMaxQubits)));
     fn<<<(unsigned)grid, kPassThreads, tma_pass_smem_bytes<WT>(A.N), ctx->stream>>>(A, map, G);
     FQ_CUDA(cudaGetLastError());
+    ctx->last_grid = (int)grid;
     prof_end(ctx, tok, pass_kind<PH, GM, EX, true>(), pass_bytes<PH, EX, true>(A.N));
     ctx->launches++;
     return FQ_OK;
 }
 
 // Launch one pass with the round schedule its target mask needs.  Passes
-// without RX (cost phase, <C>, cut diagonal) use the L0 schedule.  Passes
+// without RX (cost phase, <C>, cut diagonal) use the L0 schedule.  RX passes
 // that read and write the state run as TMA pipelines where tma_for() and
-// the tile geometry allow; write-only (layer-0) and read-only passes use
-// k_pass.
+// the tile geometry allow; every other pass uses k_pass.
 template <typename WT, int PH, int GM, int EX, bool ST>
 inline int launch_pass(fq_ctx* ctx, const PassArgs& A) {
     if constexpr (ST && PH != PH_INIT && EX != EX_DIAG && EX != EX_COSTATE) {
-        if (tma_for(PH)) {
+        if (tma_for(PH, A)) {
             alignas(64) CUtensorMap map;
             TmaGeom G;
             if (make_pass_tmap(A, &map, &G)) {
@@ -166,13 +187,8 @@ inline int launch_pass(fq_ctx* ctx, const PassArgs& A) {
     }
 }
 
-// Grid (and <C> partial count) of a pass launched by launch_pass.
-inline int pass_grid(fq_ctx* ctx, const PassArgs& A, int ph, bool st) {
-    const bool tma = st && ph != PH_INIT && tma_for(ph) && tmap_encoder() && A.sv &&
-                     ((uintptr_t)A.sv & 127) == 0 && A.l >= 3;
-    const i64 per = tma ? 1 : ctx->ctas_per_sm;
-    return (int)std::min<i64>(A.ntiles, per * ctx->num_sms);
-}
+// Grid (and <C> partial count) of the tile pass launched last.
+inline int pass_grid(fq_ctx* ctx, const PassArgs&, int, bool) { return ctx->last_grid; }
 
 // ---- dispatch entry points (one translation unit each) -------------------
 

@@ -232,38 +232,37 @@ __device__ __forceinline__ void group_sync(int g) {
     asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kPassThreads) : "memory");
 }
 
-// exchange() for one of several 256-thread groups of a CTA.
-template <int LF, int LT>
-__device__ __forceinline__ void exchange_g(double2 (&v)[kRegs], double2* buf, int gtid, int g) {
-    group_sync(g);
-#pragma unroll
-    for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(gtid, r))] = v[r];
-    group_sync(g);
-#pragma unroll
-    for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(gtid, r))];
-}
-
 // Layouts L1 and L2 both put tile bits 9..11 on the warp index, so a change
 // between them stays inside each warp's 512-amplitude region of buf (the
 // swizzle only permutes bits 0..2): a warp barrier is enough.  Such an
 // exchange must follow reads of buf in L1 or L2 (the warp's own region), as
 // every schedule here does; exchanges from or to L0 cross warps and use the
 // block barrier.
-template <int LF, int LT>
-__device__ __forceinline__ void buf_sync() {
-    if (LF != 0 && LT != 0)
-        __syncwarp();
+// PAIR: the CTA holds two 256-thread groups, each on its own tile and
+// buffer; the block barrier is then the group's named barrier.
+template <bool PAIR>
+__device__ __forceinline__ void tile_sync(int grp) {
+    if (PAIR)
+        group_sync(grp);
     else
         __syncthreads();
 }
 
-template <int LF, int LT>
+template <int LF, int LT, bool PAIR = false>
+__device__ __forceinline__ void buf_sync(int grp = 0) {
+    if (LF != 0 && LT != 0)
+        __syncwarp();
+    else
+        tile_sync<PAIR>(grp);
+}
+
+template <int LF, int LT, bool PAIR = false>
 __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid,
-                                         bool wait_readers = true) {
-    if (wait_readers) buf_sync<LF, LT>();  // previous readers of buf are done
+                                         bool wait_readers = true, int grp = 0) {
+    if (wait_readers) buf_sync<LF, LT, PAIR>(grp);  // previous readers of buf are done
 #pragma unroll
     for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
-    buf_sync<LF, LT>();
+    buf_sync<LF, LT, PAIR>(grp);
 #pragma unroll
     for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
 }
@@ -286,9 +285,9 @@ __device__ __forceinline__ i64 tile_off(int t, int l, int a) {
 // also holds the N*N weights while the kernel sets up).
 template <typename WT>
 struct PassSmem {
-    static constexpr size_t red = 0;                                // 8 double
-    static constexpr size_t ke = red + 8 * sizeof(double);          // 2 x 32 WT
-    static constexpr size_t creg = ke + 64 * sizeof(WT);            // 2 x 16 WT (L0, L1)
+    static constexpr size_t red = 0;                                // 16 double
+    static constexpr size_t ke = red + 16 * sizeof(double);         // 2 groups x 2 x 32 WT
+    static constexpr size_t creg = ke + 128 * sizeof(WT);           // 2 x 16 WT (L0, L1)
     static constexpr size_t Dm = creg + 32 * sizeof(WT);            // 24 WT
     static constexpr size_t Ru = Dm + 24 * sizeof(WT);              // 16 WT
     static constexpr size_t wf = Ru + 16 * sizeof(WT);              // kMaxFixed x kWfStride
@@ -300,10 +299,10 @@ struct PassSmem {
 };
 
 // Shared-memory bytes k_pass needs (independent of N: the weights are
-// staged in the exchange buffer).
+// staged in the exchange buffer); a paired CTA has two exchange buffers.
 template <typename WT>
-__host__ __device__ inline size_t pass_smem_bytes(int) {
-    return sizeof(double2) * kTile + PassSmem<WT>::bytes;
+__host__ __device__ inline size_t pass_smem_bytes(int, bool pair = false) {
+    return sizeof(double2) * kTile * (pair ? 2 : 1) + PassSmem<WT>::bytes;
 }
 
 // Cut value of register slot r: c_r = cbase + creg[r] + sum_k r_k g_k, so
@@ -331,7 +330,7 @@ __device__ __forceinline__ void phase_bit(double2 (&v)[kRegs], int k, double2 E)
 // Shared-memory tables of the cut decomposition for one pass geometry.
 template <typename WT>
 struct CutTables {
-    WT* ke;        // 2 x 32, double-buffered per tile: [0] = K, [1+u] = e_u
+    WT* ke;        // 2 x 32 per group, double-buffered per tile: [0] = K, [1+u] = e_u
     WT* creg;      // 16 per layout (L0, then L1): cut among the 4 register bits
     WT* Dm;        // nF: sum of weights between fixed bit m and the tile bits
     WT* Ru;        // 12: sum of weights between tile bit u and the fixed bits
@@ -496,12 +495,22 @@ __device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* sm
 // that layer's RX (GM2, A.gx2) on the same targets.  With the layer order
 // reversed every other layer, the last pass of one layer and the first of
 // the next share a tile geometry, so two sweeps become one.
-template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE>
-__global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
+//
+// PAIR (strided tiles with 128-byte rows, l = 3): 512 threads, one CTA per
+// SM, as two 256-thread groups that take the two tiles differing only in
+// physical bit 3 (tile numbers 2t and 2t+1) at the same time, each with its
+// own exchange buffer, tile constants and named barrier.  Their loads and
+// stores then meet DRAM as 256-byte rows: per-thread sweeps over 128-byte
+// rows measured 4.1-4.9 TB/s on B200 at N=30, over 256-byte rows 5.6 TB/s.
+template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
+          bool PAIR = false>
+__global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ? 1 : 2)
+    k_pass(const PassArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
-    double2* buf = reinterpret_cast<double2*>(smraw);
-    unsigned char* const sm = smraw + sizeof(double2) * kTile;
+    const int grp = PAIR ? (int)(threadIdx.x >> 8) : 0;  // the thread's group (tile of the pair)
+    double2* buf = reinterpret_cast<double2*>(smraw) + (size_t)grp * kTile;
+    unsigned char* const sm = smraw + sizeof(double2) * kTile * (PAIR ? 2 : 1);
     double* red = reinterpret_cast<double*>(sm + SM::red);
     const CutTables<WT> ct(sm);
     double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
@@ -511,23 +520,26 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
     constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
     constexpr bool INTW = sizeof(WT) == sizeof(int);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // tid, lane and warp index the thread within its group of 256.
+    const int tid = threadIdx.x & (kPassThreads - 1), lane = tid & 31, warp = tid >> 5;
     const int nmid = a - l;  // fixed bits between the row bits and the high tile bits
     // Product-tree phases: integer weights with the two-level table (nhi ==
     // 0 keeps one global-table lookup per amplitude), FP64 weights when the
     // host allows it (A.tree: small |gamma| * sum|w|, see phase_tree_ok).
     const bool tree = PH != PH_NONE && (INTW ? A.nhi > 0 : A.tree != 0);
 
-    // ---- set-up: compact weight tables of this pass's tile geometry
-    WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
+    // ---- set-up: compact weight tables of this pass's tile geometry (the
+    // tables depend on the geometry only: one copy serves both groups)
+    WT* sw = reinterpret_cast<WT*>(smraw);  // N*N weights while setting up
     if (CUT) {
         const WT* gw = reinterpret_cast<const WT*>(A.w);
-        for (int i = tid; i < N * N; i += kPassThreads) sw[i] = gw[i];
+        for (int i = threadIdx.x; i < N * N; i += blockDim.x) sw[i] = gw[i];
     }
-    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, tid, kPassThreads);
+    if (PH != PH_NONE && INTW) load_phase_tables(A, smtab, threadIdx.x, blockDim.x);
     __syncthreads();
-    if (CUT) ct.template setup<PH != PH_NONE>(sw, N, l, a, tid, A.gamma);
-    __syncthreads();  // the weights in buf are dead from here on
+    if (CUT && threadIdx.x < kPassThreads)
+        ct.template setup<PH != PH_NONE>(sw, N, l, a, tid, A.gamma);
+    __syncthreads();  // the weights in the buffer are dead from here on
 
     // Address pieces: the thread's offsets in layouts L0 and L1 and the
     // strides of the 4 register bits of each (uniform across the grid).
@@ -551,7 +563,9 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
     double acc = 0, comp = 0;  // Kahan-compensated <C> accumulator
 
     int par = 0;
-    for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
+    const i64 nunits = PAIR ? A.ntiles / 2 : A.ntiles;
+    for (i64 U = blockIdx.x; U < nunits; U += gridDim.x, par ^= 1) {
+        const i64 T = PAIR ? 2 * U + grp : U;
         const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
         double2* const p = A.sv + base + thr_off;
         double2 v[kRegs];
@@ -562,7 +576,7 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             if (LOAD) v[r] = __ldcs(p + off0(r));
             else v[r] = make_double2(0.0, 0.0);
         }
-        if (LOAD && A.pf_dist > 0 && contiguous) {
+        if (!PAIR && LOAD && A.pf_dist > 0 && contiguous) {
             // Stream this CTA's tile pf_dist strides ahead from HBM into L2
             // (one bulk prefetch).  Strided tiles are not prefetched: the
             // per-row prefetches cost more than they saved (measured on the
@@ -576,11 +590,12 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                              : "memory");
             }
         }
-        WT* const kp = ct.ke + 32 * par;  // double-buffered: no barrier for the previous readers
+        // double-buffered per group: no barrier for the previous readers
+        WT* const kp = ct.ke + 64 * grp + 32 * par;
         WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
         if (CUT) {
             ct.tile(kp, base | A.goff, nF, l, a, warp, lane);
-            __syncthreads();
+            tile_sync<PAIR>(grp);
             ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }
         // The cost phase (PH_INIT writes it, PH_MUL multiplies it in), with
@@ -625,11 +640,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
             rx_regs<G>(v, m_hi, gx, A.c, A.s);
             if (lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
             if (SC == SC_L021) {
-                exchange<0, 2>(v, buf, tid, !(first && CUT));
+                exchange<0, 2, PAIR>(v, buf, tid, !(first && CUT), grp);
                 rx_regs<G>(v, m_lo, gx, A.c, A.s);
-                exchange<2, 1>(v, buf, tid, true);
+                exchange<2, 1, PAIR>(v, buf, tid, true, grp);
             } else if (SC == SC_L01) {
-                exchange<0, 1>(v, buf, tid, !(first && CUT));
+                exchange<0, 1, PAIR>(v, buf, tid, !(first && CUT), grp);
             }
             if (SC != SC_L0) rx_regs<G>(v, m_mid, gx, A.c, A.s);
         };
@@ -660,16 +675,16 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
                     // as in L0.
                     if (lo_lane >= 0) rx_lane<G2>(v, lo_lane, A.gx2, A.c, A.s);
                     if (SC == SC_L021) {
-                        exchange<1, 2>(v, buf, tid, true);
+                        exchange<1, 2, PAIR>(v, buf, tid, true, grp);
                         rx_regs<G2>(v, m_lo, A.gx2, A.c, A.s);
-                        exchange<2, 0>(v, buf, tid, true);
+                        exchange<2, 0, PAIR>(v, buf, tid, true, grp);
                     } else {
-                        exchange<1, 0>(v, buf, tid, true);
+                        exchange<1, 0, PAIR>(v, buf, tid, true, grp);
                     }
                     rx_regs<G2>(v, m_hi, A.gx2, A.c, A.s);
                 }
             } else if (SC != SC_L0 && LAY == 0) {
-                exchange<1, 0>(v, buf, tid, true);
+                exchange<1, 0, PAIR>(v, buf, tid, true, grp);
             }
         }
         // The cut constants again for the outputs that need them (read back
@@ -715,11 +730,11 @@ __global__ void __launch_bounds__(kPassThreads, 2) k_pass(const PassArgs A) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         __syncthreads();
-        if (lane == 0) red[warp] = acc;
+        if (lane == 0) red[threadIdx.x >> 5] = acc;
         __syncthreads();
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
             double s = 0;
-            for (int w = 0; w < kPassThreads / 32; w++) s += red[w];
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
             A.partial[blockIdx.x] = s;
         }
     }

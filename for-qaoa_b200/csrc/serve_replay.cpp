@@ -160,9 +160,19 @@ void run_sequential(std::vector<Sess>& ss, int steps, bool reuse, std::vector<Re
         for (int k = 0; k < steps; k++) {
             double e;
             const double t1 = now_s();
+            // A plain call allocates its state and costate (N > 12) and frees
+            // them afterwards, inside the timed call.
+            const bool own = !reuse && s.N > 12;
+            if (own && ((st = fq_state_alloc(ctx, s.N, &sv)) || (st = fq_state_alloc(ctx, s.N, &cs))))
+                die("fq_state_alloc", st);
             st = fq_qaoa_energy_grad(ctx, sv, cs, s.N, s.P, s.graph.data(), s.g.data(),
                                      s.b.data(), &e, gg.data(), gb.data());
             if (st) die("fq_qaoa_energy_grad", st);
+            if (own) {
+                if ((st = fq_state_free(ctx, sv)) || (st = fq_state_free(ctx, cs)))
+                    die("fq_state_free", st);
+                sv = cs = nullptr;
+            }
             out.push_back(Rec{s.id, k, s.N, s.P, e, now_s() - t1, 0.0, gg, gb});
             next_angles(s.g, s.b, gg.data(), gb.data(), s.P);
         }

@@ -18,8 +18,8 @@ LIB_PATH = os.path.join(HERE, "libforqaoa.so")
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BUSY = range(7)
 
 # Kernel kinds of fq_ctx_profile (include/forqaoa.h)
-KINDS = {"layer_pass": 0, "strided_pass": 1, "cost": 2, "rx": 3, "swap": 4, "expect": 5,
-         "other": 6, "adjoint": 7}
+KINDS = {"phase_pass": 0, "mixer_pass": 1, "cost": 2, "rx": 3, "swap": 4, "expect": 5,
+         "other": 6, "adjoint": 7, "init_pass": 8}
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("libforqaoa.so not built: run `make -C for-qaoa_b200` "

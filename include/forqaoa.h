@@ -74,15 +74,17 @@ int fq_ctx_device_info(fq_ctx* ctx, int* num_sms, int* ctas_per_sm);
  * device time (ms), the launch count and the summed algorithmic HBM bytes
  * (bytes the kernel must move: 16 per amplitude read, 16 per amplitude
  * written).  Kinds: */
-#define FQ_KIND_LAYER_PASS 0    /* fused pass: cost phase + RX on 12 low qubits */
-#define FQ_KIND_STRIDED_PASS 1  /* fused pass: RX on high qubits, strided tile */
+#define FQ_KIND_PHASE_PASS 0    /* engine tile pass with a cost phase and RX: a fused
+                                   two-layer pass, or a later layer's first pass */
+#define FQ_KIND_MIXER_PASS 1    /* engine tile pass with RX only */
 #define FQ_KIND_COST 2          /* fq_cost_phase */
 #define FQ_KIND_RX 3            /* fq_rx_chunk / fq_rx_targets */
 #define FQ_KIND_SWAP 4          /* fq_swap_blocks */
 #define FQ_KIND_EXPECT 5        /* <C> / cut diagonal sweeps */
 #define FQ_KIND_OTHER 6         /* tables, reductions, permutations, small instances */
 #define FQ_KIND_ADJOINT 7       /* reverse-sweep passes over state and costate */
-#define FQ_KIND_COUNT 8
+#define FQ_KIND_INIT_PASS 8     /* engine's layer-0 pass: launch-control init, write-only */
+#define FQ_KIND_COUNT 9
 int fq_ctx_set_profiling(fq_ctx* ctx, int enable);
 int fq_ctx_profile(fq_ctx* ctx, int kind, double* total_ms, long long* launches,
                    double* bytes);
