@@ -9,16 +9,17 @@
 
 namespace fq {
 
-template <typename WT, bool PHI, int SC, int GM, int GM2>
+template <typename WT, bool PHI, int SC, int GM, int GM2, bool TURN = false>
 inline int dual_launch(fq_ctx* ctx, const PassArgs& A, double* gb, double* gg, double* gb2) {
-    auto fn = k_pass_dual<WT, PHI, SC, true, GM, GM2>;
+    auto fn = k_pass_dual<WT, PHI, SC, true, GM, GM2, TURN>;
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)dual_smem_bytes<WT>(kMaxQubits)));
     const i64 grid = std::min<i64>(A.ntiles, (i64)ctx->num_sms);
     const int tok = prof_begin(ctx);
     fn<<<(unsigned)grid, kPassThreads, dual_smem_bytes<WT>(A.N), ctx->stream>>>(A, gb, gg, gb2);
     FQ_CUDA(cudaGetLastError());
-    prof_end(ctx, tok, FQ_KIND_ADJOINT, 64.0 * (double)(1ull << A.N));
+    // The turnaround reads one vector and writes two.
+    prof_end(ctx, tok, FQ_KIND_ADJOINT, (TURN ? 48.0 : 64.0) * (double)(1ull << A.N));
     ctx->launches++;
     return FQ_OK;
 }
@@ -48,6 +49,28 @@ inline int dual_phase_dispatch(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, 
     if (gm2 == GM_NONE) return dual_sc<WT, true, GM_COT, GM_NONE>(ctx, A, gb, gg, gb2);
     if (gm2 == GM_TAN) return dual_sc<WT, true, GM_COT, GM_TAN>(ctx, A, gb, gg, gb2);
     return dual_sc<WT, true, GM_COT, GM_COT>(ctx, A, gb, gg, gb2);
+}
+
+// The turnaround pass (k_pass_dual with TURN): the forward's last pass
+// (gmf, A.gx2), lambda = C psi with <C> (partials to ge) and the reverse
+// sweep's first pass (gm, A.gx, dE/dbeta partials to gb), in one sweep.
+template <typename WT>
+inline int dual_turn_dispatch(fq_ctx* ctx, int gm, int gmf, const PassArgs& A, double* gb,
+                              double* ge) {
+    FQ_CHECK((gm == GM_TAN || gm == GM_COT) && (gmf == GM_TAN || gmf == GM_COT), FQ_ERR_INVALID,
+             "turnaround pass needs reduced gates (%d, %d)", gm, gmf);
+    auto sc = [&](auto gtag, auto ftag) -> int {
+        constexpr int G = decltype(gtag)::value, F = decltype(ftag)::value;
+        switch (schedule_for(A.tmask)) {
+            case SC_L021: return dual_launch<WT, false, SC_L021, G, F, true>(ctx, A, gb, ge, nullptr);
+            case SC_L01: return dual_launch<WT, false, SC_L01, G, F, true>(ctx, A, gb, ge, nullptr);
+            default: return dual_launch<WT, false, SC_L0, G, F, true>(ctx, A, gb, ge, nullptr);
+        }
+    };
+    using T = std::integral_constant<int, GM_TAN>;
+    using C = std::integral_constant<int, GM_COT>;
+    if (gm == GM_TAN) return gmf == GM_TAN ? sc(T(), T()) : sc(T(), C());
+    return gmf == GM_TAN ? sc(C(), T()) : sc(C(), C());
 }
 
 }  // namespace fq

@@ -8,4 +8,9 @@ int dispatch_dual_phase_fp(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, doub
     return dual_phase_dispatch<double>(ctx, gm, gm2, A, gb, gg, gb2);
 }
 
+int dispatch_dual_turn_fp(fq_ctx* ctx, int gm, int gmf, const PassArgs& A, double* gb,
+                           double* ge) {
+    return dual_turn_dispatch<double>(ctx, gm, gmf, A, gb, ge);
+}
+
 }  // namespace fq

@@ -8,4 +8,9 @@ int dispatch_dual_phase_int(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, dou
     return dual_phase_dispatch<int>(ctx, gm, gm2, A, gb, gg, gb2);
 }
 
+int dispatch_dual_turn_int(fq_ctx* ctx, int gm, int gmf, const PassArgs& A, double* gb,
+                           double* ge) {
+    return dual_turn_dispatch<int>(ctx, gm, gmf, A, gb, ge);
+}
+
 }  // namespace fq

@@ -415,7 +415,8 @@ bool fuse_enabled() {
 // instead of P * npass (11 instead of 15 at N=30, p=5).
 static int engine_forward_fused(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g,
                                 const double* gammas, const double* betas, double* energy,
-                                const std::vector<PassPlan>& plan, int& last_grid) {
+                                const std::vector<PassPlan>& plan, int& last_grid,
+                                bool skip_last) {
     const double amp0 = fq_init_amp(N);
     const int npass = (int)plan.size();
     std::vector<int> gm(P);
@@ -438,6 +439,7 @@ static int engine_forward_fused(fq_ctx* ctx, void* sv, int N, int P, const Graph
     };
     for (int p = 0; p < P; p++) {
         for (int j = (p == 0 ? 0 : 1); j < npass; j++) {
+            if (skip_last && p == P - 1 && j == npass - 1) break;
             const int idx = (p % 2 == 0) ? j : npass - 1 - j;
             PassArgs A = base_args(ctx, sv, N, g);
             A.l = plan[idx].l;
@@ -465,14 +467,28 @@ static int engine_forward_fused(fq_ctx* ctx, void* sv, int N, int P, const Graph
     return FQ_OK;
 }
 
+bool engine_fused(const GraphPrep& g, int N, int P) {
+    return fuse_enabled() && plan_layer(N).size() >= 2 && P >= 2 &&
+           (!g.integer || (engine_nhi(g) > 0 && P <= kMaxTableLayers));
+}
+
+int engine_last_pass(const GraphPrep& g, int N, int P) {
+    const int npass = (int)plan_layer(N).size();
+    return (engine_fused(g, N, P) && (P - 1) % 2 == 1) ? 0 : npass - 1;
+}
+
 int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, const double* gammas,
-                   const double* betas, double* energy) {
+                   const double* betas, double* energy, bool skip_last) {
     const double amp0 = fq_init_amp(N);
     const std::vector<PassPlan> plan = plan_layer(N);
     int last_grid = 0;
-    const bool fused = fuse_enabled() && plan.size() >= 2 && P >= 2 &&
-                       (!g.integer || (engine_nhi(g) > 0 && P <= kMaxTableLayers));
-    if (fused) FQ_TRY(engine_forward_fused(ctx, sv, N, P, g, gammas, betas, energy, plan, last_grid));
+    const bool fused = engine_fused(g, N, P);
+    FQ_CHECK(!(skip_last && (energy || plan.size() < 2)), FQ_ERR_INVALID,
+             "the forward circuit can stop before its last pass only without <C> and with two "
+             "or more passes per layer");
+    if (fused)
+        FQ_TRY(engine_forward_fused(ctx, sv, N, P, g, gammas, betas, energy, plan, last_grid,
+                                    skip_last));
     for (int p = 0; p < (fused ? 0 : P); p++) {
         int gm;
         double gx, f;
@@ -493,6 +509,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
             }
         }
         for (size_t i = 0; i < plan.size(); i++) {
+            if (skip_last && p == P - 1 && i + 1 == plan.size()) break;
             PassArgs A = base_args(ctx, sv, N, g);
             A.l = plan[i].l;
             A.a = plan[i].a;

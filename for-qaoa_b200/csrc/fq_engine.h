@@ -50,8 +50,14 @@ int reduce_to_result(fq_ctx* ctx, int n);
 int read_result(fq_ctx* ctx, double* host);
 int check_state(void* sv, int N);
 int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g);
+// The forward circuit (fq_qaoa_forward); skip_last stops before the last
+// pass of the last layer (the gradient's turnaround pass runs it).
 int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, const double* gammas,
-                   const double* betas, double* energy);
+                   const double* betas, double* energy, bool skip_last = false);
+// Whether engine_forward uses the fused two-layer schedule, and the plan
+// index of the last pass it runs.
+bool engine_fused(const GraphPrep& g, int N, int P);
+int engine_last_pass(const GraphPrep& g, int N, int P);
 
 // The N >= 13 gradient split for asynchronous use: grad_enqueue puts every
 // kernel and the final device-to-host copy of the results on ctx's stream;

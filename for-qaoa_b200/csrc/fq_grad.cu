@@ -148,15 +148,6 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
     const int npass = (int)plan.size();
     FQ_CHECK(1 + P + P * npass < kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
 
-    // Forward circuit, then lambda = C psi with <C>.
-    FQ_TRY(engine_forward(ctx, sv, N, P, g, gammas, betas, nullptr));
-    {
-        PassArgs A = base_args(ctx, sv, N, g);
-        A.sv2 = (double2*)costate;
-        FQ_TRY(dispatch_costate(ctx, g.integer, A));
-        FQ_TRY(reduce_partials(ctx, ctx->d_partial, pass_grid(ctx, A, PH_NONE, false),
-                               ctx->d_result));
-    }
     // Reverse sweep.  Layer k visits its passes in the reverse of the
     // forward order (descending plan order for even k, ascending for odd
     // k); its last pass completes the layer's mixer, so it also takes
@@ -184,6 +175,20 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             rev.push_back({k, i, last, last && fuse && k > 0});
         }
     const int nrev = (int)rev.size();
+    // Turnaround: the forward circuit's last pass, lambda = C psi with <C>
+    // and the reverse sweep's first pass share one tile geometry, so they
+    // run as one sweep (k_pass_dual with TURN) whenever the first reverse
+    // pass is an RX pass over the last forward pass's tile.  Otherwise the
+    // forward circuit runs to its end and a <C> sweep writes lambda.
+    const bool turn = !rev[0].phi && rev[0].i == engine_last_pass(g, N, P);
+    FQ_TRY(engine_forward(ctx, sv, N, P, g, gammas, betas, nullptr, turn));
+    if (!turn) {
+        PassArgs A = base_args(ctx, sv, N, g);
+        A.sv2 = (double2*)costate;
+        FQ_TRY(dispatch_costate(ctx, g.integer, A));
+        FQ_TRY(reduce_partials(ctx, ctx->d_partial, pass_grid(ctx, A, PH_NONE, false),
+                               ctx->d_result));
+    }
     const int grid = (int)std::min<i64>(1ll << (N - kTileBits), (i64)ctx->num_sms);
     const bool batched = (i64)nrev * 3 * grid <= ctx->partial_cap && 3 * nrev <= kMaxGradSums;
     const bool all_tables = g.integer && engine_nhi(g) > 0 && P <= kMaxTableLayers;
@@ -212,7 +217,13 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
         double* gb2 = gb + 2 * grid;
         const int dst_b = 1 + P + k * npass + i, dst_g = 1 + k;
         const int dst_b2 = 1 + P + (k - 1) * npass + i;
-        if (!R.phi) {
+        if (turn && q == 0) {
+            int gmf;
+            double f_unused;
+            gate_params(betas[k], gmf, A.gx2, f_unused);
+            FQ_TRY(g.integer ? dispatch_dual_turn_int(ctx, gm[k], gmf, A, gb, gg)
+                             : dispatch_dual_turn_fp(ctx, gm[k], gmf, A, gb, gg));
+        } else if (!R.phi) {
             FQ_TRY(dispatch_dual_rx(ctx, gm[k], A, gb));
         } else {
             if (g.integer && !all_tables) {
@@ -237,12 +248,15 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
             FQ_TRY(g.integer ? dispatch_dual_phase_int(ctx, gm[k], gm2, A, gb, gg, gb2)
                              : dispatch_dual_phase_fp(ctx, gm[k], gm2, A, gb, gg, gb2));
         }
+        const bool energy_here = turn && q == 0;  // <C> partials of the turnaround
         if (batched) {
             sums.dst[3 * q] = dst_b;
             if (R.phi) sums.dst[3 * q + 1] = dst_g;
+            if (energy_here) sums.dst[3 * q + 1] = 0;
             if (R.fused) sums.dst[3 * q + 2] = dst_b2;
         } else {
             FQ_TRY(reduce_partials(ctx, gb, grid, ctx->d_result + dst_b));
+            if (energy_here) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result));
             if (R.phi) FQ_TRY(reduce_partials(ctx, gg, grid, ctx->d_result + dst_g));
             if (R.fused) FQ_TRY(reduce_partials(ctx, gb2, grid, ctx->d_result + dst_b2));
         }

@@ -38,6 +38,8 @@
 // each amplitude costs a few integer adds.
 #pragma once
 
+#include <cuda.h>
+
 #include <type_traits>
 
 #include "fq_common.cuh"
@@ -98,6 +100,8 @@ struct PassArgs {
                      // the factor (f^2) it gains with every reduced rotation
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
+    int pf_tma;      // strided tiles: box kind of the tensor map k_pass prefetches
+                     // with (TG_ROWS or TG_ROWS8), -1 = no tensor prefetch
     i64 goff;        // shard of a larger state: global index of sv[0] (enters cut values only)
     int* err;        // device error flag (bounded waits that gave up)
 };
@@ -141,8 +145,17 @@ __device__ __forceinline__ double2 int_phase(const PassArgs& A, const double2* s
     return __ldg(A.ptab + ti);
 }
 
-// Swizzled slot of tile index t in the exchange buffer.
+// Swizzled slot of tile index t in a 64 KB exchange buffer (the TMA pass,
+// whose landed stage is the buffer): bits 0..2 XORed with bits 4..6.
 __device__ __forceinline__ int xslot(int t) { return t ^ ((t >> 4) & 7); }
+// Padded slot of tile index t (k_pass, k_pass_dual): one empty 16-byte slot
+// after every 16, so every quarter-warp's accesses fall in distinct banks in
+// all three layouts, and -- unlike the XOR swizzle -- the slots of a
+// thread's 16 registers are its first slot plus constants (the register
+// bits have strides of 16 or more tile indices, or sit in bits 0..3 of a
+// multiple of 16), which the compiler folds into the access instructions.
+__device__ __forceinline__ int pslot(int t) { return t + (t >> 4); }
+constexpr int kXTile = kTile + kTile / 16;  // slots of a padded buffer
 
 template <int GM>
 __device__ __forceinline__ void rx_pair(double2& p, double2& q, double g, double c, double s) {
@@ -256,15 +269,40 @@ __device__ __forceinline__ void buf_sync(int grp = 0) {
         tile_sync<PAIR>(grp);
 }
 
-template <int LF, int LT, bool PAIR = false>
+// First padded slot of a thread's registers in layout L, taken through an
+// empty volatile asm so that it is recomputed (two or three integer ops) at
+// each exchange instead of being kept in a register across the tile loop.
+// The slot of register r is this plus pslot(lay_index<L>(0, r)), a constant:
+// pslot is additive over the thread part and the register part of a tile
+// index in every layout.
+template <int L>
+__device__ __forceinline__ int pbase(int tid) {
+    int b = pslot(lay_index<L>(tid, 0));
+    asm volatile("" : "+r"(b));
+    return b;
+}
+
+template <int LF, int LT, bool PAIR = false, bool PAD = true>
 __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid,
                                          bool wait_readers = true, int grp = 0) {
     if (wait_readers) buf_sync<LF, LT, PAIR>(grp);  // previous readers of buf are done
+    if (PAD) {
+        double2* const wb = buf + pbase<LF>(tid);
 #pragma unroll
-    for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
+        for (int r = 0; r < kRegs; r++) wb[pslot(lay_index<LF>(0, r))] = v[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < kRegs; r++) buf[xslot(lay_index<LF>(tid, r))] = v[r];
+    }
     buf_sync<LF, LT, PAIR>(grp);
+    if (PAD) {
+        const double2* const rb = buf + pbase<LT>(tid);
 #pragma unroll
-    for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
+        for (int r = 0; r < kRegs; r++) v[r] = rb[pslot(lay_index<LT>(0, r))];
+    } else {
+#pragma unroll
+        for (int r = 0; r < kRegs; r++) v[r] = buf[xslot(lay_index<LT>(tid, r))];
+    }
 }
 
 constexpr int kWfStride = 21;  // row stride of the compact weight tables (odd: no bank conflicts)
@@ -281,7 +319,7 @@ __device__ __forceinline__ i64 tile_off(int t, int l, int a) {
     return (i64)(t & ((1 << l) - 1)) | ((i64)(t >> l) << a);
 }
 
-// Shared-memory layout of k_pass after the 64 KB exchange buffer (which
+// Shared-memory layout of k_pass after its padded exchange buffer (which
 // also holds the N*N weights while the kernel sets up).
 template <typename WT>
 struct PassSmem {
@@ -302,7 +340,7 @@ struct PassSmem {
 // staged in the exchange buffer); a paired CTA has two exchange buffers.
 template <typename WT>
 __host__ __device__ inline size_t pass_smem_bytes(int, bool pair = false) {
-    return sizeof(double2) * kTile * (pair ? 2 : 1) + PassSmem<WT>::bytes;
+    return sizeof(double2) * kXTile * (pair ? 2 : 1) + PassSmem<WT>::bytes;
 }
 
 // Cut value of register slot r: c_r = cbase + creg[r] + sum_k r_k g_k, so
@@ -502,15 +540,19 @@ __device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* sm
 // own exchange buffer, tile constants and named barrier.  Their loads and
 // stores then meet DRAM as 256-byte rows: per-thread sweeps over 128-byte
 // rows measured 4.1-4.9 TB/s on B200 at N=30, over 256-byte rows 5.6 TB/s.
+//
+// The tile one grid-stride ahead is prefetched into L2 while this one is
+// loaded: one bulk prefetch for a contiguous tile, one tensor prefetch
+// through pfm (the tile as a TMA box, A.pf_tma >= 0) for a strided one.
 template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
           bool PAIR = false>
 __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ? 1 : 2)
-    k_pass(const PassArgs A) {
+    k_pass(const PassArgs A, const __grid_constant__ CUtensorMap pfm) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
     const int grp = PAIR ? (int)(threadIdx.x >> 8) : 0;  // the thread's group (tile of the pair)
-    double2* buf = reinterpret_cast<double2*>(smraw) + (size_t)grp * kTile;
-    unsigned char* const sm = smraw + sizeof(double2) * kTile * (PAIR ? 2 : 1);
+    double2* buf = reinterpret_cast<double2*>(smraw) + (size_t)grp * kXTile;
+    unsigned char* const sm = smraw + sizeof(double2) * kXTile * (PAIR ? 2 : 1);
     double* red = reinterpret_cast<double*>(sm + SM::red);
     const CutTables<WT> ct(sm);
     double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
@@ -576,18 +618,35 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             if (LOAD) v[r] = __ldcs(p + off0(r));
             else v[r] = make_double2(0.0, 0.0);
         }
-        if (!PAIR && LOAD && A.pf_dist > 0 && contiguous) {
-            // Stream this CTA's tile pf_dist strides ahead from HBM into L2
-            // (one bulk prefetch).  Strided tiles are not prefetched: the
-            // per-row prefetches cost more than they saved (measured on the
-            // fused strided pass: 12.2 ms with, 11.2 ms without).
-            const i64 T2 = T + (i64)A.pf_dist * gridDim.x;
-            if (T2 < A.ntiles && tid == 0) {
-                const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
-                               ((T2 >> nmid) << (a + kTileBits - l));
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
-                             "r"((unsigned)(kTile * sizeof(double2)))
-                             : "memory");
+        if (LOAD && A.pf_dist > 0 && tid == 0) {
+            // Stream this group's tile pf_dist grid-strides ahead from HBM
+            // into L2: a contiguous tile in one bulk prefetch, a strided
+            // one as its TMA box (per-thread row prefetches of a strided
+            // tile cost more than they saved: 12.2 against 11.2 ms on the
+            // fused strided pass at N=30).
+            const i64 U2 = U + (i64)A.pf_dist * gridDim.x;
+            if (U2 < nunits) {
+                const i64 T2 = PAIR ? 2 * U2 + grp : U2;
+                const int c_lo = (int)(T2 & ((1ll << nmid) - 1)), c_hi = (int)(T2 >> nmid);
+                if (contiguous) {
+                    const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
+                                   ((T2 >> nmid) << (a + kTileBits - l));
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
+                                 "r"((unsigned)(kTile * sizeof(double2)))
+                                 : "memory");
+                } else if (A.pf_tma == 1) {  // TG_ROWS: {16, 2^(l-3), 1, 2^(12-l), 1}
+                    asm volatile(
+                        "cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, "
+                        "%5}];" ::"l"(&pfm),
+                        "r"(0), "r"(0), "r"(c_lo), "r"(0), "r"(c_hi)
+                        : "memory");
+                } else if (A.pf_tma == 2) {  // TG_ROWS8: {16, 1, 32, 16, 1}
+                    asm volatile(
+                        "cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, "
+                        "%5}];" ::"l"(&pfm),
+                        "r"(0), "r"(c_lo), "r"(0), "r"(0), "r"(c_hi)
+                        : "memory");
+                }
             }
         }
         // double-buffered per group: no barrier for the previous readers

@@ -93,26 +93,32 @@ template <int LF, int LT>
 __device__ __forceinline__ void exchange_dual(double2 (&v)[kRegs], double2 (&w)[kRegs],
                                               double2* buf, int tid, bool wait_readers = true) {
     if (wait_readers) buf_sync<LF, LT>();  // previous readers of buf are done
+    {
+        double2* const wb = buf + pbase<LF>(tid);
 #pragma unroll
-    for (int r = 0; r < kRegs; r++) {
-        const int sl = xslot(lay_index<LF>(tid, r));
-        buf[sl] = v[r];
-        buf[kTile + sl] = w[r];
+        for (int r = 0; r < kRegs; r++) {
+            const int sl = pslot(lay_index<LF>(0, r));
+            wb[sl] = v[r];
+            wb[kXTile + sl] = w[r];
+        }
     }
     buf_sync<LF, LT>();
+    {
+        const double2* const rb = buf + pbase<LT>(tid);
 #pragma unroll
-    for (int r = 0; r < kRegs; r++) {
-        const int sl = xslot(lay_index<LT>(tid, r));
-        v[r] = buf[sl];
-        w[r] = buf[kTile + sl];
+        for (int r = 0; r < kRegs; r++) {
+            const int sl = pslot(lay_index<LT>(0, r));
+            v[r] = rb[sl];
+            w[r] = rb[kXTile + sl];
+        }
     }
 }
 
-// Shared memory: two 64 KB exchange buffers (the weights are staged in them
-// while the kernel sets up), then the tables of k_pass.
+// Shared memory: two padded exchange buffers (the weights are staged in
+// them while the kernel sets up), then the tables of k_pass.
 template <typename WT>
 __host__ __device__ inline size_t dual_smem_bytes(int) {
-    return 2 * sizeof(double2) * kTile + PassSmem<WT>::bytes + 24 * sizeof(double);
+    return 2 * sizeof(double2) * kXTile + PassSmem<WT>::bytes + 24 * sizeof(double);
 }
 
 // RX(-beta) in reduced form GM (A.gx = t or u, A.f2 = f^2, A.sc0 = scale of
@@ -130,13 +136,22 @@ __host__ __device__ inline size_t dual_smem_bytes(int) {
 // The next tile of both vectors is prefetched into L2 while the current one
 // is computed (one CTA per SM cannot hide the HBM latency of its loads
 // otherwise).
-template <typename WT, bool PHI, int SC, bool ST, int GM, int GM2 = GM_NONE>
+//
+// TURN: the turnaround of the gradient, three sweeps in one: the forward
+// circuit's last pass (RX(+beta) of the last layer, reduced form GM2 with
+// A.gx2, on the tile's targets), the costate lambda = C psi of the final
+// state with <C> (Kahan sums to gg), and the reverse sweep's first pass
+// (RX(-beta), GM with A.gx, from scale A.sc0, dE/dbeta partials to gb).
+// Only psi is read (the state before the last forward pass); both vectors
+// are written as the reverse sweep's first pass would write them: 32 B
+// per amplitude instead of 32 + 48 + 64.
+template <typename WT, bool PHI, int SC, bool ST, int GM, int GM2 = GM_NONE, bool TURN = false>
 __global__ void __launch_bounds__(kPassThreads, 1)
     k_pass_dual(const PassArgs A, double* gb, double* gg, double* gb2) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
     double2* buf = reinterpret_cast<double2*>(smraw);
-    unsigned char* const sm = smraw + 2 * sizeof(double2) * kTile;
+    unsigned char* const sm = smraw + 2 * sizeof(double2) * kXTile;
     const CutTables<WT> ct(sm);
     double2* smtab = reinterpret_cast<double2*>(sm + SM::smtab);
     double* red = reinterpret_cast<double*>(sm + SM::bytes);  // 24: the three partials
@@ -144,12 +159,13 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const int nF = N - kTileBits;
     const int nmid = a - l;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr bool CUT = PHI;
+    constexpr bool CUT = PHI || TURN;
     constexpr bool INTW = sizeof(WT) == sizeof(int);
-    constexpr bool FUSED = GM2 != GM_NONE;
+    constexpr bool FUSED = !TURN && GM2 != GM_NONE;
     static_assert(PHI || !FUSED, "a fused adjoint pass carries its layer's phase");
+    static_assert(!(PHI && TURN), "the turnaround pass carries no phase");
     constexpr int LP = SC == SC_L0 ? 0 : 1;  // layout after the first rounds
-    constexpr int LAY = FUSED ? 0 : LP;       // layout of the stores
+    constexpr int LAY = (FUSED || TURN) ? 0 : LP;  // layout of the stores
 
     WT* sw = reinterpret_cast<WT*>(buf);  // N*N weights while setting up
     if (CUT) {
@@ -175,6 +191,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const unsigned m_hi = (A.tmask >> 8) & 15u, m_mid = (A.tmask >> 4) & 15u, m_lo = A.tmask & 15u;
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double accb = 0, accg = 0, accb2 = 0;
+    double ecomp = 0;  // Kahan compensation of <C> (TURN, in accg)
     const double g = A.gx, f2 = A.f2;
 
     int par = 0;
@@ -187,13 +204,13 @@ __global__ void __launch_bounds__(kPassThreads, 1)
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
                 v[r] = __ldcs(A.sv + o + offr(r, b8, b9, b10, b11));
-                w[r] = __ldcs(A.sv2 + o + offr(r, b8, b9, b10, b11));
+                if (!TURN) w[r] = __ldcs(A.sv2 + o + offr(r, b8, b9, b10, b11));
             }
         }
         if (T + gridDim.x < A.ntiles) {
             const i64 b2 = tile_base(T + gridDim.x);
             if (contiguous) {
-                if (tid < 2)
+                if (tid < (TURN ? 1 : 2))
                     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(
                                      (tid ? A.sv2 : A.sv) + b2),
                                  "r"((unsigned)(kTile * sizeof(double2)))
@@ -202,7 +219,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 for (int j = tid; j < (1 << (kTileBits - pf_step)); j += kPassThreads) {
                     const i64 o = b2 + tile_off(j << pf_step, l, a);
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv + o) : "memory");
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv2 + o) : "memory");
+                    if (!TURN) asm volatile("prefetch.global.L2 [%0];" ::"l"(A.sv2 + o) : "memory");
                 }
             }
         }
@@ -218,6 +235,49 @@ __global__ void __launch_bounds__(kPassThreads, 1)
         // this tile's first barrier (the leading barrier of its first
         // exchange, a block barrier).
         double sc = A.sc0;
+        if constexpr (TURN) {
+            // The forward's last pass on psi alone: L0 -> (L2 ->) L1.
+            const double gf = A.gx2;
+            rx_regs<GM2>(v, m_hi, gf, 0.0, 0.0);
+            if (lo_lane >= 0) rx_lane<GM2>(v, lo_lane, gf, 0.0, 0.0);
+            if (SC == SC_L021) {
+                exchange<0, 2>(v, buf, xt, true);
+                rx_regs<GM2>(v, m_lo, gf, 0.0, 0.0);
+                exchange<2, 1>(v, buf, xt, true);
+            } else if (SC == SC_L01) {
+                exchange<0, 1>(v, buf, xt, true);
+            }
+            if (SC != SC_L0) rx_regs<GM2>(v, m_mid, gf, 0.0, 0.0);
+            // The final state: <C> and lambda = C psi (cut constants of layout LP).
+            if (SC == SC_L0) __syncthreads();  // kp written by warps 0 and 1
+            WT cbase, g0, g1, g2, g3;
+            ct.template consts<LP>(kp, tid, cbase, g0, g1, g2, g3);
+            const WT* crg = ct.creg + 16 * LP;
+            double te = 0;
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                              ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
+                const double c = (double)cr;
+                te = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), c, te);
+                w[r] = make_double2(c * v[r].x, c * v[r].y);
+            }
+            const double y = te - ecomp;
+            const double t2 = accg + y;
+            ecomp = (t2 - accg) - y;
+            accg = t2;
+            // The reverse sweep's first pass, back to L0.
+            if (SC != SC_L0) rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
+            if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
+            if (SC == SC_L021) {
+                exchange_dual<1, 2>(v, w, buf, xt, true);
+                rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
+                exchange_dual<2, 0>(v, w, buf, xt, true);
+            } else if (SC == SC_L01) {
+                exchange_dual<1, 0>(v, w, buf, xt, true);
+            }
+            rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
+        } else {
         rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
         if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
         if (SC == SC_L021) {
@@ -311,6 +371,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 rx_regs_dual<GM2>(v, w, m_hi, g2x, f2b, sc2, accb2);
             }
         }
+        }  // !TURN
         if (ST) {
             if (LAY == 0) {
                 const i64 o = opaque(base + thr_off);
@@ -352,7 +413,7 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             sb2 += red[16 + k];
         }
         gb[blockIdx.x] = sb;
-        if (PHI) gg[blockIdx.x] = sg;
+        if (PHI || TURN) gg[blockIdx.x] = sg;
         if (FUSED) gb2[blockIdx.x] = sb2;
     }
 }

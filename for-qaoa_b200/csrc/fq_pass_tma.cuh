@@ -264,15 +264,15 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
             if (lo_lane >= 0) rx_lane<GM>(v, lo_lane, A.gx, A.c, A.s);
             if (SC == SC_L021) {
-                exchange<0, 2>(v, buf, tid);
+                exchange<0, 2, false, false>(v, buf, tid);
                 rx_regs<GM>(v, m_lo, A.gx, A.c, A.s);
-                exchange<2, 1>(v, buf, tid);
+                exchange<2, 1, false, false>(v, buf, tid);
             } else if (SC == SC_L01) {
-                exchange<0, 1>(v, buf, tid);
+                exchange<0, 1, false, false>(v, buf, tid);
             }
             if (SC != SC_L0) {
                 rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
-                if (LAY == 0) exchange<1, 0>(v, buf, tid);
+                if (LAY == 0) exchange<1, 0, false, false>(v, buf, tid);
             }
         }
         if (EX == EX_ENERGY) {
