@@ -210,16 +210,17 @@ static int choose_lrows(int N) {
     return best;
 }
 
-// One layer's passes: the contiguous tile 0..11, then strided tiles
-// bringing the next 12 - lrows qubits on chip each (the last strided pass
-// widens its rows when fewer qubits remain); with three or more passes the
-// first strided pass leads and the contiguous one moves to second place.
-// The first pass of a layer carries its cost phase (layer 0: the
-// launch-control init), and the fused schedule runs the first and last
-// passes of consecutive layers as one sweep, so the passes that fuse are the
-// strided ones and the contiguous pass (four exchanges when fused, two alone)
-// runs alone in the middle: on B200 at N=30, p=5, 59.5-59.7 layers/s against
-// 57.2-57.6 with the contiguous pass first (A/B in one call).
+// One layer's passes: the contiguous tile 0..11 and strided tiles bringing
+// the next 12 - lrows qubits on chip each (the last strided pass widens its
+// rows when fewer qubits remain).  The first pass of a layer carries its
+// cost phase (layer 0: the launch-control init), and the fused schedule
+// runs the first and last passes of consecutive layers as one sweep, so
+// with three or more passes the contiguous pass (four exchanges when fused,
+// two alone) goes second and never fuses: on B200 at N=30, p=5, 59.5-59.7
+// layers/s against 57.2-57.6 with it first (A/B in one call).  The strided
+// passes over the highest qubits lead and the one over the lowest closes
+// each layer: an odd circuit then ends on the faster of the two strided
+// geometries (61.2-61.8 against 60.3-61.0 layers/s, A/B in one call).
 std::vector<PassPlan> plan_layer(int N) {
     std::vector<PassPlan> v;
     v.push_back({kTileBits, kTileBits, (1u << kTileBits) - 1});
@@ -230,7 +231,10 @@ std::vector<PassPlan> plan_layer(int N) {
         v.push_back({l, q, ((1u << k) - 1) << l});
         q += k;
     }
-    if (v.size() >= 3) std::swap(v[0], v[1]);
+    if (v.size() >= 3) {  // [last strided, contiguous, ..., first strided]
+        std::swap(v[0], v[v.size() - 1]);
+        std::swap(v[1], v[v.size() - 1]);
+    }
     return v;
 }
 

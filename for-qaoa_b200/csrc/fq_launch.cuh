@@ -42,37 +42,16 @@ inline double pass_bytes(int N) {
 // on the TMA pipeline instead.
 inline bool pair_ok(const PassArgs& A) { return A.l == 3 && A.a > A.l && A.ntiles >= 2; }
 
-inline bool make_pass_tmap(const PassArgs& A, CUtensorMap* map, TmaGeom* G);
-
-// EXPERIMENT (FQ_TPF=0 turns it off): L2 tensor prefetch of strided tiles.
-inline bool tpf_enabled() {
-    static int m = -1;
-    if (m < 0) {
-        const char* e = getenv("FQ_TPF");
-        m = e ? atoi(e) : 1;
-    }
-    return m != 0;
-}
-
 template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
           bool PAIR = false>
-inline int launch_ldg_as(fq_ctx* ctx, const PassArgs& A0) {
+inline int launch_ldg_as(fq_ctx* ctx, const PassArgs& A) {
     auto fn = k_pass<WT, PH, GM, EX, ST, SC, GM2, PAIR>;
-    PassArgs A = A0;
-    alignas(64) CUtensorMap pfm;
-    memset(&pfm, 0, sizeof(pfm));
-    A.pf_tma = -1;
-    constexpr bool LOADS = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
-    if (LOADS && A.pf_dist > 0 && A.l < kTileBits && tpf_enabled()) {
-        TmaGeom G;
-        if (make_pass_tmap(A, &pfm, &G) && G.kind != TG_CONTIG) A.pf_tma = G.kind;
-    }
     const size_t smem = pass_smem_bytes<WT>(A.N, PAIR);
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const i64 units = PAIR ? A.ntiles / 2 : A.ntiles;
     const i64 grid = std::min<i64>(units, (i64)(PAIR ? 1 : ctx->ctas_per_sm) * ctx->num_sms);
     const int tok = prof_begin(ctx);
-    fn<<<(unsigned)grid, PAIR ? 2 * kPassThreads : kPassThreads, smem, ctx->stream>>>(A, pfm);
+    fn<<<(unsigned)grid, PAIR ? 2 * kPassThreads : kPassThreads, smem, ctx->stream>>>(A);
     FQ_CUDA(cudaGetLastError());
     ctx->last_grid = (int)grid;
     prof_end(ctx, tok, pass_kind<PH, GM, EX, ST>(), pass_bytes<PH, EX, ST>(A.N));

@@ -95,9 +95,7 @@ int launch_na_pass(const PassArgs& A, int grid, cudaStream_t st) {
     auto fn = k_pass<WT, PH_NONE, GM_NONE, EX_ENERGY, false, SC_L0>;
     FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)pass_smem_bytes<WT>(kMaxQubits)));
-    CUtensorMap none;  // no prefetch in this read-only sweep (A.pf_dist == 0)
-    memset(&none, 0, sizeof(none));
-    fn<<<grid, kPassThreads, pass_smem_bytes<WT>(A.N), st>>>(A, none);
+    fn<<<grid, kPassThreads, pass_smem_bytes<WT>(A.N), st>>>(A);
     FQ_CUDA(cudaGetLastError());
     return FQ_OK;
 }

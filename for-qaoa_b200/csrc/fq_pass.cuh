@@ -38,8 +38,6 @@
 // each amplitude costs a few integer adds.
 #pragma once
 
-#include <cuda.h>
-
 #include <type_traits>
 
 #include "fq_common.cuh"
@@ -100,8 +98,6 @@ struct PassArgs {
                      // the factor (f^2) it gains with every reduced rotation
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
-    int pf_tma;      // strided tiles: box kind of the tensor map k_pass prefetches
-                     // with (TG_ROWS or TG_ROWS8), -1 = no tensor prefetch
     i64 goff;        // shard of a larger state: global index of sv[0] (enters cut values only)
     int* err;        // device error flag (bounded waits that gave up)
 };
@@ -540,14 +536,10 @@ __device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* sm
 // own exchange buffer, tile constants and named barrier.  Their loads and
 // stores then meet DRAM as 256-byte rows: per-thread sweeps over 128-byte
 // rows measured 4.1-4.9 TB/s on B200 at N=30, over 256-byte rows 5.6 TB/s.
-//
-// The tile one grid-stride ahead is prefetched into L2 while this one is
-// loaded: one bulk prefetch for a contiguous tile, one tensor prefetch
-// through pfm (the tile as a TMA box, A.pf_tma >= 0) for a strided one.
 template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
           bool PAIR = false>
 __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ? 1 : 2)
-    k_pass(const PassArgs A, const __grid_constant__ CUtensorMap pfm) {
+    k_pass(const PassArgs A) {
     extern __shared__ __align__(16) unsigned char smraw[];
     using SM = PassSmem<WT>;
     const int grp = PAIR ? (int)(threadIdx.x >> 8) : 0;  // the thread's group (tile of the pair)
@@ -618,35 +610,20 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             if (LOAD) v[r] = __ldcs(p + off0(r));
             else v[r] = make_double2(0.0, 0.0);
         }
-        if (LOAD && A.pf_dist > 0 && tid == 0) {
-            // Stream this group's tile pf_dist grid-strides ahead from HBM
-            // into L2: a contiguous tile in one bulk prefetch, a strided
-            // one as its TMA box (per-thread row prefetches of a strided
-            // tile cost more than they saved: 12.2 against 11.2 ms on the
-            // fused strided pass at N=30).
-            const i64 U2 = U + (i64)A.pf_dist * gridDim.x;
-            if (U2 < nunits) {
-                const i64 T2 = PAIR ? 2 * U2 + grp : U2;
-                const int c_lo = (int)(T2 & ((1ll << nmid) - 1)), c_hi = (int)(T2 >> nmid);
-                if (contiguous) {
-                    const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
-                                   ((T2 >> nmid) << (a + kTileBits - l));
-                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
-                                 "r"((unsigned)(kTile * sizeof(double2)))
-                                 : "memory");
-                } else if (A.pf_tma == 1) {  // TG_ROWS: {16, 2^(l-3), 1, 2^(12-l), 1}
-                    asm volatile(
-                        "cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, "
-                        "%5}];" ::"l"(&pfm),
-                        "r"(0), "r"(0), "r"(c_lo), "r"(0), "r"(c_hi)
-                        : "memory");
-                } else if (A.pf_tma == 2) {  // TG_ROWS8: {16, 1, 32, 16, 1}
-                    asm volatile(
-                        "cp.async.bulk.prefetch.tensor.5d.L2.global.tile [%0, {%1, %2, %3, %4, "
-                        "%5}];" ::"l"(&pfm),
-                        "r"(0), "r"(c_lo), "r"(0), "r"(0), "r"(c_hi)
-                        : "memory");
-                }
+        if (!PAIR && LOAD && A.pf_dist > 0 && contiguous) {
+            // Stream this CTA's tile pf_dist strides ahead from HBM into L2
+            // (one bulk prefetch).  Strided tiles are not prefetched: per-
+            // thread row prefetches cost more than they saved (12.2 against
+            // 11.2 ms on the fused strided pass at N=30), and so did a tensor
+            // prefetch of the tile as a TMA box (61.5 against 58.1-61.0
+            // layers/s at N=30, p=5; A/B in one call).
+            const i64 T2 = T + (i64)A.pf_dist * gridDim.x;
+            if (T2 < A.ntiles && tid == 0) {
+                const i64 b2 = ((T2 & ((1ll << nmid) - 1)) << l) |
+                               ((T2 >> nmid) << (a + kTileBits - l));
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(A.sv + b2),
+                             "r"((unsigned)(kTile * sizeof(double2)))
+                             : "memory");
             }
         }
         // double-buffered per group: no barrier for the previous readers
