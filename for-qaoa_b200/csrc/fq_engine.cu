@@ -678,10 +678,19 @@ static int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double
         A.s = s;
         FQ_TRY(dispatch_rx_full(ctx, A));
     }
+    // Targets above bit 11: strided tiles whose high bits are a window of
+    // k qubits, in 9-qubit windows; a window spans only as many qubits as
+    // its targets do (at least one), so few targets, such as the one or two
+    // a sharded state swaps in per layer, leave the rows wide (2^(12-k)
+    // contiguous amplitudes) and the pass streams at the copy rate.
     unsigned long long rest = mask & ~0xFFFull;
-    const int k = std::min(kTileBits - 3, N - kTileBits);
+    const int kmax = std::min(kTileBits - 3, N - kTileBits);
     while (rest) {
         const int t0 = __builtin_ctzll(rest);
+        int hi = t0;
+        for (int t = t0; t < t0 + kmax && t < N; t++)
+            if ((rest >> t) & 1ull) hi = t;
+        const int k = hi - t0 + 1;
         const int a = std::min(t0, N - k);
         PassArgs A = base_args(ctx, sv, N, g);
         A.l = kTileBits - k;

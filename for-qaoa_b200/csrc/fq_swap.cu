@@ -24,20 +24,25 @@ struct SwapArgs {
     int N, o, i, k;
     int eb;      // element bits kept inside a tile row (<= o)
     int a;       // sub-tile bits taken from each block
-    int nob;     // "other" bits: [eb,o), [o+k,i), [i+k,N)
+    int m;       // bits [o+k, o+k+m) also kept inside a row (only when a == k)
+    int nob;     // "other" bits: [eb,o), [o+k+m,i), [i+k,N)
     i64 npairs;  // sub-tile pairs (I <= J)
     i64 nitems;
 };
 
 __global__ void __launch_bounds__(256) k_swap_blocks(const SwapArgs S) {
     extern __shared__ __align__(16) double2 sm[];
-    const int rowlen = 1 << (S.a + S.eb);  // contiguous amplitudes per row
+    // A row holds the element bits e (eb), the out-block low bits x (a) and
+    // the free bits f above the out block (m): 2^(eb+a+m) amplitudes,
+    // contiguous when o <= 6 and a == k.
+    const int rowlen = 1 << (S.a + S.eb + S.m);
     const int rows = 1 << S.a;
     const int stride = rowlen + 1;  // padding keeps the transposed read conflict-free
     const int tsize = rows * rowlen;
     double2* t0 = sm;
     double2* t1 = sm + rows * stride;
-    const int n1 = S.o - S.eb, n2 = S.i - S.o - S.k;
+    const int n1 = S.o - S.eb, n2 = S.i - S.o - S.k - S.m;
+    const int xeb = S.a + S.eb;  // bits of (e, x) in a row index
     for (i64 item = blockIdx.x; item < S.nitems; item += gridDim.x) {
         const i64 oi = item & ((1ll << S.nob) - 1);
         const i64 p = item >> S.nob;
@@ -46,7 +51,7 @@ __global__ void __launch_bounds__(256) k_swap_blocks(const SwapArgs S) {
         while ((J + 1) * (J + 2) / 2 <= p) J++;
         const i64 I = p - J * (J + 1) / 2;
         const i64 base = ((oi & ((1ll << n1) - 1)) << S.eb) |
-                         (((oi >> n1) & ((1ll << n2) - 1)) << (S.o + S.k)) |
+                         (((oi >> n1) & ((1ll << n2) - 1)) << (S.o + S.k + S.m)) |
                          ((oi >> (n1 + n2)) << (S.i + S.k));
         const i64 bIJ = base | (I << (S.o + S.a)) | (J << (S.i + S.a));
         const i64 bJI = base | (J << (S.o + S.a)) | (I << (S.i + S.a));
@@ -55,19 +60,21 @@ __global__ void __launch_bounds__(256) k_swap_blocks(const SwapArgs S) {
         // out-block low bits x and the element bits e (contiguous when o <= 6,
         // runs of 2^eb = 64 amplitudes otherwise).
         for (int idx = threadIdx.x; idx < tsize; idx += 256) {
-            const int y = idx >> (S.a + S.eb), xe = idx & (rowlen - 1);
-            const i64 off = (xe & ((1 << S.eb) - 1)) + ((i64)(xe >> S.eb) << S.o) +
-                            ((i64)y << S.i);
+            const int y = idx >> (xeb + S.m), xe = idx & (rowlen - 1);
+            const int f = xe >> xeb, x = (xe >> S.eb) & ((1 << S.a) - 1);
+            const i64 off = (xe & ((1 << S.eb) - 1)) + ((i64)x << S.o) +
+                            ((i64)f << (S.o + S.k)) + ((i64)y << S.i);
             t0[y * stride + xe] = __ldcs(S.sv + bIJ + off);
             if (!diag) t1[y * stride + xe] = __ldcs(S.sv + bJI + off);
         }
         __syncthreads();
         // Element (x, y) of (I, J) lands at (y, x) of (J, I), and vice versa.
         for (int idx = threadIdx.x; idx < tsize; idx += 256) {
-            const int yd = idx >> (S.a + S.eb), xe = idx & (rowlen - 1);
-            const int xd = xe >> S.eb, e = xe & ((1 << S.eb) - 1);
-            const int src = xd * stride + (yd << S.eb) + e;
-            const i64 off = e + ((i64)xd << S.o) + ((i64)yd << S.i);
+            const int yd = idx >> (xeb + S.m), xe = idx & (rowlen - 1);
+            const int f = xe >> xeb, xd = (xe >> S.eb) & ((1 << S.a) - 1);
+            const int e = xe & ((1 << S.eb) - 1);
+            const int src = xd * stride + (f << xeb) + (yd << S.eb) + e;
+            const i64 off = e + ((i64)xd << S.o) + ((i64)f << (S.o + S.k)) + ((i64)yd << S.i);
             __stcs(S.sv + bJI + off, t0[src]);
             if (!diag) __stcs(S.sv + bIJ + off, t1[src]);
         }
@@ -98,11 +105,19 @@ extern "C" int fq_swap_blocks(fq_ctx* ctx, void* sv, int N, int swap_out, int sw
     S.k = num_swap;
     S.eb = std::min(swap_out, 6);
     S.a = std::min(num_swap, std::max(0, (10 - S.eb) / 2));
-    S.nob = (swap_out - S.eb) + (swap_in - swap_out - num_swap) + (N - swap_in - num_swap);
+    // A small block (the whole block in one sub-tile) leaves rows short;
+    // the free bits right above the out block fill them up to 2^10
+    // amplitudes per sub-tile (a swap of 2-qubit blocks at bit 0 took 7.9 ms
+    // at N=26 with 4-amplitude rows).
+    S.m = S.a == num_swap ? std::max(0, std::min(swap_in - swap_out - num_swap,
+                                                  10 - 2 * S.a - S.eb))
+                          : 0;
+    S.nob = (swap_out - S.eb) + (swap_in - swap_out - num_swap - S.m) +
+            (N - swap_in - num_swap);
     const i64 M = 1ll << (num_swap - S.a);
     S.npairs = M * (M + 1) / 2;
     S.nitems = S.npairs << S.nob;
-    const size_t smem = sizeof(double2) * 2 * (1 << S.a) * ((1 << (S.a + S.eb)) + 1);
+    const size_t smem = sizeof(double2) * 2 * (1 << S.a) * ((1 << (S.a + S.eb + S.m)) + 1);
     const i64 grid = std::min<i64>(S.nitems, (i64)ctx->num_sms * 8);
     const int tok = prof_begin(ctx);
     k_swap_blocks<<<(unsigned)grid, 256, smem, ctx->stream>>>(S);
