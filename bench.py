@@ -254,11 +254,11 @@ KIND_KERNELS = {
 
 def ncu_traffic_per_launch(kind, args):
     """DRAM bytes (read + write) per launch of a pass kind at N=30 from the
-    committed ncu summary (profiles/pass_kernels_n30_p5.md), or None (other
+    committed ncu summary (profiles/engine_passes_n30_p5.md), or None (other
     sizes have no committed figure)."""
     if not is_headline(args):
         return None
-    p = os.path.join(ROOT, "profiles", "pass_kernels_n30_p5.md")
+    p = os.path.join(ROOT, "profiles", "engine_passes_n30_p5.md")
     try:
         m = re.search(r"traffic_bytes_per_launch\[%s\]:\s*([0-9.eE+]+)" % kind, open(p).read())
         return float(m.group(1)) if m else None
