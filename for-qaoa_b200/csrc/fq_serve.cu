@@ -1,7 +1,9 @@
 // fq_serve.cu -- continuous batching of QAOA energy+gradient requests.
 //
-// One scheduler thread owns the device work; requests are admitted as
-// resources free up and their work overlaps on the GPU:
+// Requests are admitted as resources free up and their work overlaps on the
+// GPU; a scheduler thread runs the small-instance batches and every lane has
+// a thread of its own, so the ~30 kernel launches of a larger request are
+// issued by its lane's thread, in parallel with the other lanes':
 //   - small instances (N <= 12) are packed one per CTA into launches of
 //     k_small_jobs (the whole instance in shared memory); two batches can be
 //     in flight on their own streams, and a batch takes every small request
@@ -72,6 +74,7 @@ struct Lane {
     cudaEvent_t done = nullptr;
     bool busy = false;
     Req cur;
+    std::thread th;  // the lane's own thread: takes requests, launches, completes them
 };
 
 constexpr int kBatchCap = 4096;           // small instances per launch
@@ -126,7 +129,7 @@ struct fq_server {
     std::deque<Req> small_q, large_q;      // guarded by mu
     std::vector<fq_result> done;           // guarded by mu
     std::mutex mu;
-    std::condition_variable cv_done, cv_work;
+    std::condition_variable cv_done, cv_work, cv_lane;
     std::thread worker;
     bool stop = false;
     uint64_t next_ticket = 1;
@@ -374,6 +377,46 @@ struct fq_server {
         L.busy = false;
     }
 
+    // ---- lane threads ----------------------------------------------------------
+    // A lane takes the next runnable large request (pick_large), enqueues its
+    // kernels on the lane's stream, waits for its event (polling, so that
+    // sixteen lanes do not hold sixteen cores in a blocking wait) and
+    // completes it.  It leaves once the server stops and no large request is
+    // queued.
+    void lane_loop(Lane& L) {
+        cudaSetDevice(device);
+        while (true) {
+            Req r;
+            Session* s = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                while (!pick_large(r, s)) {
+                    if (stop && large_q.empty()) return;
+                    cv_lane.wait_for(lk, std::chrono::milliseconds(2));
+                }
+            }
+            const int st = start_large(L, r, *s);
+            if (st != FQ_OK) {
+                fail(st);
+                end_step(r.session);
+                finish(r, st, nullptr, nullptr, nullptr, now_s());
+                cv_lane.notify_all();
+                continue;
+            }
+            while (true) {
+                const cudaError_t q = cudaEventQuery(L.done);
+                if (q == cudaSuccess) break;
+                if (q != cudaErrorNotReady) {
+                    cudaGetLastError();
+                    break;  // grad_collect reports the failure
+                }
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+            complete_large(L);
+            cv_lane.notify_all();  // the session may have a next step queued
+        }
+    }
+
     // ---- scheduler loop -----------------------------------------------------
     void loop() {
         cudaSetDevice(device);
@@ -398,34 +441,9 @@ struct fq_server {
                 }
                 pending |= B.busy;
             }
-            for (auto& L : lanes) {
-                if (L.busy && cudaEventQuery(L.done) == cudaSuccess) {
-                    complete_large(L);
-                    worked = true;
-                }
-                if (!L.busy) {
-                    Req r;
-                    Session* s = nullptr;
-                    bool have;
-                    {
-                        std::lock_guard<std::mutex> lk(mu);
-                        have = pick_large(r, s);
-                    }
-                    if (have) {
-                        const int st = start_large(L, r, *s);
-                        if (st != FQ_OK) {
-                            fail(st);
-                            end_step(r.session);
-                            finish(r, st, nullptr, nullptr, nullptr, now_s());
-                        }
-                        worked = true;
-                    }
-                }
-                pending |= L.busy;
-            }
             if (worked) continue;
             std::unique_lock<std::mutex> lk(mu);
-            if (stop && small_q.empty() && large_q.empty() && !pending) break;
+            if (stop && small_q.empty() && !pending) break;
             if (pending) {
                 lk.unlock();
                 std::this_thread::sleep_for(std::chrono::microseconds(10));
@@ -464,7 +482,7 @@ int fq_server_create(int device, double hbm_budget_bytes, int lanes, fq_server**
         if (st == FQ_OK &&
             cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
             st = FQ_ERR_CUDA;
-        S->lanes.push_back(L);
+        S->lanes.push_back(std::move(L));
     }
     for (auto& B : S->batches) {
         if (st != FQ_OK) break;
@@ -497,20 +515,25 @@ int fq_server_create(int device, double hbm_budget_bytes, int lanes, fq_server**
         return st;
     }
     S->worker = std::thread([S] { S->loop(); });
+    for (auto& L : S->lanes) {
+        Lane* lp = &L;
+        L.th = std::thread([S, lp] { S->lane_loop(*lp); });
+    }
     *out = S;
     return FQ_OK;
 }
 
 int fq_server_destroy(fq_server* S) {
     if (!S) return FQ_OK;
-    if (S->worker.joinable()) {
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            S->stop = true;
-            S->cv_work.notify_all();
-        }
-        S->worker.join();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv_work.notify_all();
+        S->cv_lane.notify_all();
     }
+    if (S->worker.joinable()) S->worker.join();
+    for (auto& L : S->lanes)
+        if (L.th.joinable()) L.th.join();
     cudaSetDevice(S->device);
     for (auto& L : S->lanes)
         if (L.st) cudaStreamSynchronize(L.st);
@@ -582,6 +605,7 @@ int fq_server_submit(fq_server* S, const fq_request* q, uint64_t* ticket) {
         S->large_q.push_back(std::move(r));
     }
     S->cv_work.notify_one();
+    S->cv_lane.notify_one();
     return FQ_OK;
 }
 

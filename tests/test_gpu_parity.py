@@ -135,6 +135,9 @@ def test_rx_chunk_rejects_bad_targets(ctx, fq):
     (12, 0, 6, 6), (14, 0, 5, 5), (16, 2, 9, 4), (13, 0, 12, 1), (20, 0, 10, 10),
     (18, 7, 11, 3), (20, 0, 12, 8), (15, 3, 8, 5), (22, 0, 11, 11), (21, 9, 18, 3),
     (10, 0, 1, 1), (24, 0, 12, 12),
+    # small blocks whose sub-tile rows take in the free bits above the out
+    # block (the reference's last swap of a layer, e.g. swap(0, 24, 2) at N=26)
+    (16, 0, 10, 2), (20, 0, 18, 2), (14, 1, 7, 3), (18, 0, 14, 4), (26, 0, 24, 2),
 ])
 def test_swap_blocks_vs_oracle(ctx, oracle, n, out, inn, k):
     rng = np.random.default_rng(n * 31 + k)
