@@ -192,13 +192,27 @@ __global__ void __launch_bounds__(kPassThreads, 1)
     const int lo_lane = (SC != SC_L021 && m_lo) ? __ffs(m_lo) - 1 : -1;
     double accb = 0, accg = 0, accb2 = 0;
     double ecomp = 0;  // Kahan compensation of <C> (TURN, in accg)
+    // Fused passes end in layout L0 and copy the next tile of both vectors
+    // into the buffer early, as k_pass's fused passes do (on B200 for K_26,
+    // p=10: 22.25-22.27 against 22.45-22.56 ms of adjoint passes per
+    // evaluation, A/B in one call).
+    constexpr bool CPF = FUSED && ST && (SC != SC_L0);
+    bool have_next = false;
     const double g = A.gx, f2 = A.f2;
 
     int par = 0;
     for (i64 T = blockIdx.x; T < A.ntiles; T += gridDim.x, par ^= 1) {
         const i64 base = tile_base(T);
         double2 v[kRegs], w[kRegs];
-        {
+        if (CPF && have_next) {  // copied in during the previous tile (see below)
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            const double2* const own = buf + pbase<0>(tid);
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) {
+                v[r] = own[pslot(lay_index<0>(0, r))];
+                w[r] = own[kXTile + pslot(lay_index<0>(0, r))];
+            }
+        } else {
             const i64 o = opaque(base + thr_off);
             const i64 b8 = opaque(s8), b9 = opaque(s9), b10 = opaque(s10), b11 = opaque(s11);
 #pragma unroll
@@ -367,6 +381,32 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                     exchange_dual<2, 0>(v, w, buf, xt, true);
                 } else if (SC == SC_L01) {
                     exchange_dual<1, 0>(v, w, buf, xt, true);
+                }
+                if (CPF) {
+                    // Each thread's L0 slots are its own until the next
+                    // tile's first exchange: copy its part of the next tile
+                    // of both vectors there now.
+                    have_next = T + gridDim.x < A.ntiles;
+                    if (have_next) {
+                        const i64 o = opaque(tile_base(T + gridDim.x) + thr_off);
+                        const i64 b8 = opaque(s8), b9 = opaque(s9), b10 = opaque(s10),
+                                  b11 = opaque(s11);
+                        const unsigned dst =
+                            (unsigned)__cvta_generic_to_shared(buf + pbase<0>(tid));
+#pragma unroll
+                        for (int r = 0; r < kRegs; r++) {
+                            const unsigned d = dst + (unsigned)(16 * pslot(lay_index<0>(0, r)));
+                            const i64 off = o + offr(r, b8, b9, b10, b11);
+                            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d),
+                                         "l"(A.sv + off)
+                                         : "memory");
+                            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                                             d + (unsigned)(16 * kXTile)),
+                                         "l"(A.sv2 + off)
+                                         : "memory");
+                        }
+                        asm volatile("cp.async.commit_group;" ::: "memory");
+                    }
                 }
                 rx_regs_dual<GM2>(v, w, m_hi, g2x, f2b, sc2, accb2);
             }
