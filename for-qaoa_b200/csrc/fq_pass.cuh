@@ -188,9 +188,17 @@ __device__ __forceinline__ void rx_regs(double2 (&v)[kRegs], unsigned m4, double
     }
 }
 
+// One amplitude of an RX pair from its own value m and its partner's q (the
+// gate is symmetric in the pair: self' = a*self - i*b*partner).
+template <int GM>
+__device__ __forceinline__ double2 rx_self(double2 m, double2 q, double g, double c, double s) {
+    if (GM == GM_TAN) return make_double2(fma(g, q.y, m.x), fma(-g, q.x, m.y));
+    if (GM == GM_COT) return make_double2(fma(g, m.x, q.y), fma(g, m.y, -q.x));
+    return make_double2(m.x * c + q.y * s, m.y * c - q.x * s);
+}
+
 // RX on a qubit held in lane bit j: every lane updates its own amplitude
-// from its partner's (the gate is symmetric in the pair: self' = a*self -
-// i*b*partner).
+// from its partner's.
 template <int GM>
 __device__ __forceinline__ void rx_lane(double2 (&v)[kRegs], int j, double g, double c, double s) {
     const unsigned lm = 1u << j;
@@ -199,17 +207,7 @@ __device__ __forceinline__ void rx_lane(double2 (&v)[kRegs], int j, double g, do
         double2 q;
         q.x = __shfl_xor_sync(0xffffffffu, v[r].x, lm);
         q.y = __shfl_xor_sync(0xffffffffu, v[r].y, lm);
-        const double2 m = v[r];
-        if (GM == GM_TAN) {
-            v[r].x = fma(g, q.y, m.x);
-            v[r].y = fma(-g, q.x, m.y);
-        } else if (GM == GM_COT) {
-            v[r].x = fma(g, m.x, q.y);
-            v[r].y = fma(g, m.y, -q.x);
-        } else {
-            v[r].x = m.x * c + q.y * s;
-            v[r].y = m.y * c - q.x * s;
-        }
+        v[r] = rx_self<GM>(v[r], q, g, c, s);
     }
 }
 
@@ -301,6 +299,36 @@ __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int 
     }
 }
 
+// exchange<LF, LT> that also applies RX on the qubit of lane bit j (a
+// single target among tile bits 0..3, which is lane bit j in layouts L0 and
+// L1 alike): each thread reads its own slots and its partner lane's
+// (tid ^ 2^j) and combines them as rx_lane does, 16 more 16-byte shared
+// loads in place of rx_lane's 64 shuffles.  The rotation then takes effect
+// after the exchange instead of before it, which is the same state: it acts
+// on another qubit than the register rounds around it.  The closing warp
+// barrier keeps a partner's slots unwritten until both lanes have read them,
+// whatever the caller writes next.  On B200 at N=30 the layer-0 pass takes
+// 5.16-5.29 ms with it against 5.39-5.42 with rx_lane; the fused passes
+// measured no faster with it and keep rx_lane (A/B in one call).
+template <int LF, int LT, int GM, bool PAIR = false>
+__device__ __forceinline__ void exchange_lane(double2 (&v)[kRegs], double2* buf, int tid,
+                                              bool wait_readers, int grp, int j, double g,
+                                              double c, double s) {
+    if (wait_readers) buf_sync<LF, LT, PAIR>(grp);
+    double2* const wb = buf + pbase<LF>(tid);
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) wb[pslot(lay_index<LF>(0, r))] = v[r];
+    buf_sync<LF, LT, PAIR>(grp);
+    const double2* const rb = buf + pbase<LT>(tid);
+    const double2* const qb = buf + pbase<LT>(tid ^ (1 << j));
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) {
+        const int o = pslot(lay_index<LT>(0, r));
+        v[r] = rx_self<GM>(rb[o], qb[o], g, c, s);
+    }
+    __syncwarp();
+}
+
 constexpr int kWfStride = 21;  // row stride of the compact weight tables (odd: no bank conflicts)
 static_assert(kWfStride >= kMaxFixed, "compact weight rows hold every fixed bit");
 
@@ -343,22 +371,30 @@ __host__ __device__ inline size_t pass_smem_bytes(int, bool pair = false) {
 // its phase factors as phase(c_r) = P * Q_r * prod_k E_k^(r_k) with
 // P = phase(cbase), Q_r = z^creg[r] (per pass, shared memory) and
 // E_k = z^g_k, z = exp(i*gamma): 5 table lookups (or sincos) per thread and
-// tile instead of 16.  Applied in stages to keep few values live: first
-// P * Q_r on every slot (PH_INIT writes it, PH_MUL multiplies it in,
-// src/rzz.cu:153-154), then E_k on the slots with bit k set.
+// tile instead of 16.  The products run over four groups of four slots:
+// B_q = P * E2^(q&1) * E3^(q>>1), then B_q {1, E0, E1, E0 E1} for the
+// group's slots, each times Q_r: 48 complex products per thread where
+// multiplying P * Q_r in and then E_k into the slots with bit k set takes
+// 64 (on B200 at N=30, p=5, fused passes: 8.73-8.96 against 9.12-9.21 ms
+// in one call, 9.46-9.49 against 9.63-9.68 in another, on a box with lower
+// clocks).  PH_INIT writes the phase, PH_MUL multiplies it in
+// (src/rzz.cu:153-154).
 template <int PH>
-__device__ __forceinline__ void phase_base(double2 (&v)[kRegs], double2 P, const double2* qtab) {
+__device__ __forceinline__ void phase_tree(double2 (&v)[kRegs], double2 P, const double2* qt,
+                                           double2 E0, double2 E1, double2 E2, double2 E3) {
+    const double2 E01 = cmul(E0, E1);
+    const double2 B1 = cmul(P, E2);
 #pragma unroll
-    for (int r = 0; r < kRegs; r++) {
-        const double2 ph = cmul(P, qtab[r]);
-        v[r] = (PH == PH_INIT) ? ph : cmul(v[r], ph);
+    for (int q = 0; q < 4; q++) {
+        const double2 B = q == 0 ? P : q == 1 ? B1 : q == 2 ? cmul(P, E3) : cmul(B1, E3);
+        const double2 T[4] = {B, cmul(B, E0), cmul(B, E1), cmul(B, E01)};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = 4 * q + i;
+            const double2 ph = cmul(T[i], qt[r]);
+            v[r] = (PH == PH_INIT) ? ph : cmul(v[r], ph);
+        }
     }
-}
-
-__device__ __forceinline__ void phase_bit(double2 (&v)[kRegs], int k, double2 E) {
-#pragma unroll
-    for (int r = 0; r < kRegs; r++)
-        if ((r >> k) & 1) v[r] = cmul(v[r], E);
 }
 
 // Shared-memory tables of the cut decomposition for one pass geometry.
@@ -659,11 +695,8 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             if (tree) {
                 double2 P = phase_of<WT>(A, smtab, cb);
                 if (INTW && PH == PH_INIT) P = make_double2(P.x * A.scale, P.y * A.scale);
-                phase_base<PH>(v, P, qt);
-                phase_bit(v, 0, zpow<WT>(A, smtab, h0));
-                phase_bit(v, 1, zpow<WT>(A, smtab, h1));
-                phase_bit(v, 2, zpow<WT>(A, smtab, h2));
-                phase_bit(v, 3, zpow<WT>(A, smtab, h3));
+                phase_tree<PH>(v, P, qt, zpow<WT>(A, smtab, h0), zpow<WT>(A, smtab, h1),
+                               zpow<WT>(A, smtab, h2), zpow<WT>(A, smtab, h3));
             } else {
 #pragma unroll
                 for (int r = 0; r < kRegs; r++) {
@@ -690,13 +723,17 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
         auto rx_rounds = [&](auto gm_tag, double gx, bool first) {
             constexpr int G = decltype(gm_tag)::value;
             rx_regs<G>(v, m_hi, gx, A.c, A.s);
-            if (lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
+            if ((SC == SC_L0 || GM2 != GM_NONE) && lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
             if (SC == SC_L021) {
                 exchange<0, 2, PAIR>(v, buf, tid, !(first && CUT), grp);
                 rx_regs<G>(v, m_lo, gx, A.c, A.s);
                 exchange<2, 1, PAIR>(v, buf, tid, true, grp);
             } else if (SC == SC_L01) {
-                exchange<0, 1, PAIR>(v, buf, tid, !(first && CUT), grp);
+                if (GM2 == GM_NONE && lo_lane >= 0)
+                    exchange_lane<0, 1, G, PAIR>(v, buf, tid, !(first && CUT), grp, lo_lane, gx,
+                                                 A.c, A.s);
+                else
+                    exchange<0, 1, PAIR>(v, buf, tid, !(first && CUT), grp);
             }
             if (SC != SC_L0) rx_regs<G>(v, m_mid, gx, A.c, A.s);
         };
