@@ -242,6 +242,7 @@ int fq_ctx_destroy(fq_ctx* c) {
     cudaFree(c->d_result);
     cudaFree(c->d_err);
     cudaFree(c->d_scratch);
+    cudaFree(c->d_tcut);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->h_result) cudaFreeHost(c->h_result);
     if (c->stage_evt) cudaEventDestroy(c->stage_evt);

@@ -19,6 +19,8 @@ struct fq_ctx {
     double* d_result = nullptr;   // small device results (kResultWords)
     unsigned char* d_scratch = nullptr;  // small-instance job data (kScratchBytes)
     int* d_err = nullptr;         // kernels' error flag (nonzero: a bounded wait gave up)
+    void* d_tcut = nullptr;       // per-tile cut constants of the engine's passes (grown on demand)
+    size_t tcut_bytes = 0;
     int partial_cap = 0;
     // Pinned host staging (uploads of weights and small tables).
     unsigned char* h_stage = nullptr;

@@ -398,6 +398,66 @@ int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g) {
     return FQ_OK;
 }
 
+// Cut constants of every tile of each plan geometry (k_tile_cuts, one
+// launch) in ctx->d_tcut, grown on demand: tabs[i] serves plan[i].  Below
+// N = 21 (512 tiles) and without the buffer (a failed allocation) tabs
+// stays null and the passes compute the constants per tile, as they do for
+// shards and the read-only <C> pass.
+// The table is 64 B per tile (128 B with FP64 weights), 1/1024 of the
+// state per geometry; it replaces per-tile work on two warps of each tile
+// and the barrier after it.  On B200 at N=30, p=5, with the layer-0 pass
+// alternating its exchanges: layer-0 pass 5.26-5.32 against 5.66-5.78 ms,
+// fused passes 9.27-9.34 against 9.62-9.66, the circuit 79.1-79.6 against
+// 80.4-80.8 ms (A/B in one call).
+static int tile_cut_tables(fq_ctx* ctx, const GraphPrep& g, int N,
+                           const std::vector<PassPlan>& plan, std::vector<const void*>& tabs) {
+    tabs.assign(plan.size(), nullptr);
+    if (N < 21 || plan.size() > 4) return FQ_OK;
+    const size_t wt = g.integer ? sizeof(int) : sizeof(double);
+    const i64 ntiles = 1ll << (N - kTileBits);
+    const size_t per = (size_t)ntiles * kTcutStride * wt;
+    const size_t need = per * plan.size();
+    if (need > ctx->tcut_bytes) {
+        if (ctx->d_tcut) {
+            FQ_CUDA(cudaStreamSynchronize(ctx->stream));
+            FQ_CUDA(cudaFree(ctx->d_tcut));
+            ctx->d_tcut = nullptr;
+            ctx->tcut_bytes = 0;
+        }
+        if (cudaMalloc(&ctx->d_tcut, need) != cudaSuccess) {
+            cudaGetLastError();  // clear the allocation failure
+            ctx->d_tcut = nullptr;
+            return FQ_OK;
+        }
+        ctx->tcut_bytes = need;
+    }
+    const int grid = (int)std::min<i64>((ntiles + 7) / 8, (i64)ctx->num_sms * 4);
+    const size_t smem = g.integer ? tcut_smem_bytes<int>(N) : tcut_smem_bytes<double>(N);
+    if (g.integer)
+        FQ_CUDA(cudaFuncSetAttribute(k_tile_cuts<int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    else
+        FQ_CUDA(cudaFuncSetAttribute(k_tile_cuts<double>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TcutGeoms G;
+    memset(&G, 0, sizeof(G));
+    for (size_t i = 0; i < plan.size(); i++) {
+        G.l[i] = plan[i].l;
+        G.a[i] = plan[i].a;
+    }
+    const dim3 grid2(grid, (unsigned)plan.size());
+    if (g.integer)
+        k_tile_cuts<int><<<grid2, kPassThreads, smem, ctx->stream>>>((const int*)ctx->d_w, N, G,
+                                                                     ntiles, (int*)ctx->d_tcut);
+    else
+        k_tile_cuts<double><<<grid2, kPassThreads, smem, ctx->stream>>>(
+            (const double*)ctx->d_w, N, G, ntiles, (double*)ctx->d_tcut);
+    FQ_CUDA(cudaGetLastError());
+    ctx->launches++;
+    for (size_t i = 0; i < plan.size(); i++) tabs[i] = (char*)ctx->d_tcut + i * per;
+    return FQ_OK;
+}
+
 bool fuse_enabled() {
     static int m = -1;
     if (m < 0) {
@@ -419,7 +479,8 @@ bool fuse_enabled() {
 // instead of P * npass (11 instead of 15 at N=30, p=5).
 static int engine_forward_fused(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g,
                                 const double* gammas, const double* betas, double* energy,
-                                const std::vector<PassPlan>& plan, int& last_grid,
+                                const std::vector<PassPlan>& plan,
+                                const std::vector<const void*>& tcut, int& last_grid,
                                 bool skip_last) {
     const double amp0 = fq_init_amp(N);
     const int npass = (int)plan.size();
@@ -449,6 +510,7 @@ static int engine_forward_fused(fq_ctx* ctx, void* sv, int N, int P, const Graph
             A.l = plan[idx].l;
             A.a = plan[idx].a;
             A.tmask = plan[idx].tmask;
+            A.tcut = tcut[idx];
             A.gx = gx[p];
             const bool last_of_layer = j == npass - 1;
             int ph = PH_NONE;
@@ -490,9 +552,11 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
     FQ_CHECK(!(skip_last && (energy || plan.size() < 2)), FQ_ERR_INVALID,
              "the forward circuit can stop before its last pass only without <C> and with two "
              "or more passes per layer");
+    std::vector<const void*> tcut;
+    FQ_TRY(tile_cut_tables(ctx, g, N, plan, tcut));
     if (fused)
-        FQ_TRY(engine_forward_fused(ctx, sv, N, P, g, gammas, betas, energy, plan, last_grid,
-                                    skip_last));
+        FQ_TRY(engine_forward_fused(ctx, sv, N, P, g, gammas, betas, energy, plan, tcut,
+                                    last_grid, skip_last));
     for (int p = 0; p < (fused ? 0 : P); p++) {
         int gm;
         double gx, f;
@@ -518,6 +582,7 @@ int engine_forward(fq_ctx* ctx, void* sv, int N, int P, const GraphPrep& g, cons
             A.l = plan[i].l;
             A.a = plan[i].a;
             A.tmask = plan[i].tmask;
+            A.tcut = tcut[i];
             A.gx = gx;
             if (nhi > 0) set_table_args(A, g, gammas[p], scale);
             if (all_tables) A.ptab = ctx->d_ptab + (size_t)p * kTableStride;

@@ -99,6 +99,10 @@ struct PassArgs {
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
     i64 goff;        // shard of a larger state: global index of sv[0] (enters cut values only)
+    // Cut constants of every tile of this pass's geometry, kTcutStride WT per
+    // tile (K, then e_0..e_11; k_tile_cuts), or null: each tile computes its
+    // own (CutTables::tile, warps 0 and 1, then a barrier).
+    const void* tcut;
     int* err;        // device error flag (bounded waits that gave up)
 };
 
@@ -522,6 +526,32 @@ struct CutTables {
         }
     }
 
+    // K and e_u of the tile at `base` into out (one warp): tile()'s two
+    // warps' work in the same order, so the values are the same.
+    __device__ void tile_warp(WT* out, i64 base, int nF, int l, int a, int lane) const {
+        const int zi = lane < nF ? (int)((base >> fixed_phys(lane, l, a)) & 1) : 0;
+        const unsigned F = __ballot_sync(0xffffffffu, zi);
+        WT h = 0;
+        if (lane < nF) {
+            if (zi) h = Dm[lane];
+            const WT* row = wf + lane * kWfStride;
+#pragma unroll
+            for (int j = 1; j < kMaxFixed; j++)
+                if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi)) h += row[j];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+        if (lane == 0) out[0] = h;
+        if (lane < kTileBits) {
+            WT e = Ru[lane];
+            const WT* row = wu + lane * kWfStride;
+#pragma unroll
+            for (int j = 0; j < kMaxFixed; j++)
+                if (j < nF && ((F >> j) & 1u)) e -= 2 * row[j];
+            out[1 + lane] = e;
+        }
+    }
+
     // cb = cut value of the thread's register slot 0, g_k = change of the
     // cut when register bit k is set; slot r has c_r = cb + creg[r] +
     // sum_k r_k g_k.
@@ -539,6 +569,41 @@ struct CutTables {
         g3 = tc[4 * kPassThreads + tid] + kp[1 + rbit(L, 3)];
     }
 };
+
+// Cut constants of every tile of up to four pass geometries (blockIdx.y
+// picks one) for the tile passes to read instead of computing them per
+// tile: out[y * ntiles * kTcutStride + T * kTcutStride] = K, then
+// e_0..e_11 (CutTables::tile).  256 threads set up the tables, then each
+// warp takes tiles.  Shared memory: the N*N weights, rounded up to 16
+// bytes, then PassSmem<WT>.
+constexpr int kTcutStride = 16;
+struct TcutGeoms {
+    int l[4], a[4];
+};
+template <typename WT>
+__host__ __device__ inline size_t tcut_smem_bytes(int N) {
+    return ((N * N * sizeof(WT) + 15) & ~(size_t)15) + PassSmem<WT>::bytes;
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(kPassThreads) k_tile_cuts(const WT* w, int N, TcutGeoms G,
+                                                            i64 ntiles, WT* out) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int l = G.l[blockIdx.y], a = G.a[blockIdx.y];
+    out += (i64)blockIdx.y * ntiles * kTcutStride;
+    WT* sw = reinterpret_cast<WT*>(smraw);
+    const CutTables<WT> ct(smraw + ((N * N * sizeof(WT) + 15) & ~(size_t)15));
+    for (int i = threadIdx.x; i < N * N; i += kPassThreads) sw[i] = w[i];
+    __syncthreads();
+    ct.template setup<false>(sw, N, l, a, threadIdx.x, 0.0);
+    __syncthreads();
+    const int nF = N - kTileBits, nmid = a - l, lane = threadIdx.x & 31;
+    const int wpb = kPassThreads / 32;
+    for (i64 T = (i64)blockIdx.x * wpb + (threadIdx.x >> 5); T < ntiles; T += (i64)gridDim.x * wpb) {
+        const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
+        ct.tile_warp(out + T * kTcutStride, base, nF, l, a, lane);
+    }
+}
 
 // z^d with z = exp(i*gamma): the two-level table (integer weights) or sincos.
 template <typename WT>
@@ -587,6 +652,9 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
     const int N = A.N, l = A.l, a = A.a;
     const int nF = N - kTileBits;
     constexpr bool CUT = (PH != PH_NONE) || (EX != EX_NONE);
+    // Passes with a phase or rotations may read their tiles' cut constants
+    // from A.tcut (the read-only <C> pass always computes them per tile).
+    constexpr bool TCUT = CUT && (PH != PH_NONE || GM != GM_NONE);
     constexpr bool LOAD = (PH != PH_INIT) && (ST || EX == EX_ENERGY || EX == EX_COSTATE);
     constexpr bool ACC = (EX == EX_ENERGY || EX == EX_COSTATE);
     constexpr bool INTW = sizeof(WT) == sizeof(int);
@@ -643,6 +711,16 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
     // passes 9.56-9.61 against 9.91-10.15 ms, A/B in one call).
     constexpr bool CPF = (GM2 != GM_NONE) && LOAD && ST && (SC != SC_L0);
     bool have_next = false;  // this thread's part of the tile is in buf
+    // Write-only layer-0 passes reading table constants alternate the
+    // direction of their exchange from tile to tile (L0 -> L1 on even
+    // iterations, L1 -> L0 on odd ones, the phase and rounds in the matching
+    // layouts): each thread then writes only slots that it, or its partner
+    // lane behind exchange_lane's warp barrier, read last, so no exchange
+    // needs a leading barrier and a tile takes one barrier.
+    constexpr bool ALT = PH == PH_INIT && GM2 == GM_NONE && SC == SC_L01 && EX == EX_NONE &&
+                         GM != GM_NONE && TCUT;
+    const bool alt = ALT && A.tcut != nullptr;
+    const bool skip_lead = (CUT && !(TCUT && A.tcut)) || CPF || alt;
     for (i64 U = blockIdx.x; U < nunits; U += gridDim.x, par ^= 1) {
         const i64 T = PAIR ? 2 * U + grp : U;
         const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
@@ -678,13 +756,27 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
                              : "memory");
             }
         }
-        // double-buffered per group: no barrier for the previous readers
-        WT* const kp = ct.ke + 64 * grp + 32 * par;
+        // The tile's cut constants: from the table (kp in global memory), or
+        // computed by warps 0 and 1 into shared memory (double-buffered per
+        // group: no barrier for the previous readers) and a barrier.
+        const WT* kp = ct.ke + 64 * grp + 32 * par;
         WT cbase = 0, g0 = 0, g1 = 0, g2 = 0, g3 = 0;
         if (CUT) {
-            ct.tile(kp, base | A.goff, nF, l, a, warp, lane);
-            tile_sync<PAIR>(grp);
-            ct.consts(kp, tid, cbase, g0, g1, g2, g3);
+            if (TCUT && A.tcut) {
+                kp = reinterpret_cast<const WT*>(A.tcut) + T * kTcutStride;
+                // The next tile's constants into L1 now: the passes' sweeps
+                // evict the table from L2, and a miss on it would stall the
+                // next tile's phase.
+                const i64 Tn = T + (PAIR ? 2 * (i64)gridDim.x : (i64)gridDim.x);
+                if (tid == 0 && Tn < A.ntiles)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(
+                                     reinterpret_cast<const WT*>(A.tcut) + Tn * kTcutStride)
+                                 : "memory");
+            } else {
+                ct.tile(ct.ke + 64 * grp + 32 * par, base | A.goff, nF, l, a, warp, lane);
+                tile_sync<PAIR>(grp);
+            }
+            if (!(alt && par)) ct.consts(kp, tid, cbase, g0, g1, g2, g3);
         }
         // The cost phase (PH_INIT writes it, PH_MUL multiplies it in), with
         // the registers in layout LL (0 or 1) and that layout's constants.
@@ -718,28 +810,45 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             }
         };
         // RX rounds on the tile's targets, from layout L0 to L1 (or L0 with
-        // SC_L0).  first: the buffer's previous readers are already past a
-        // barrier (the cut barrier), so the first exchange skips its own.
+        // SC_L0).  first: the tile's first exchange skips its leading barrier
+        // when the buffer's previous readers are already past one (the cut
+        // barrier), or when the thread writes only slots that no other
+        // thread reads after the previous tile's last barrier: its own L0
+        // slots in a fused pass, whose previous tile ended by reading them.
         auto rx_rounds = [&](auto gm_tag, double gx, bool first) {
             constexpr int G = decltype(gm_tag)::value;
             rx_regs<G>(v, m_hi, gx, A.c, A.s);
             if ((SC == SC_L0 || GM2 != GM_NONE) && lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
             if (SC == SC_L021) {
-                exchange<0, 2, PAIR>(v, buf, tid, !(first && CUT), grp);
+                exchange<0, 2, PAIR>(v, buf, tid, !(first && skip_lead), grp);
                 rx_regs<G>(v, m_lo, gx, A.c, A.s);
                 exchange<2, 1, PAIR>(v, buf, tid, true, grp);
             } else if (SC == SC_L01) {
                 if (GM2 == GM_NONE && lo_lane >= 0)
-                    exchange_lane<0, 1, G, PAIR>(v, buf, tid, !(first && CUT), grp, lo_lane, gx,
+                    exchange_lane<0, 1, G, PAIR>(v, buf, tid, !(first && skip_lead), grp, lo_lane, gx,
                                                  A.c, A.s);
                 else
-                    exchange<0, 1, PAIR>(v, buf, tid, !(first && CUT), grp);
+                    exchange<0, 1, PAIR>(v, buf, tid, !(first && skip_lead), grp);
             }
             if (SC != SC_L0) rx_regs<G>(v, m_mid, gx, A.c, A.s);
         };
         constexpr bool FUSED = GM2 != GM_NONE;
         using L0t = std::integral_constant<int, 0>;
         using L1t = std::integral_constant<int, 1>;
+        if (ALT && alt && par) {  // the odd iteration of an alternating pass (see ALT)
+            WT cb, h0, h1, h2, h3;
+            ct.template consts<1>(kp, tid, cb, h0, h1, h2, h3);
+            apply_phase(L1t(), cb, h0, h1, h2, h3);
+            rx_regs<GM>(v, m_mid, A.gx, A.c, A.s);
+            if (lo_lane >= 0)
+                exchange_lane<1, 0, GM, PAIR>(v, buf, tid, false, grp, lo_lane, A.gx, A.c, A.s);
+            else
+                exchange<1, 0, PAIR>(v, buf, tid, false, grp);
+            rx_regs<GM>(v, m_hi, A.gx, A.c, A.s);
+#pragma unroll
+            for (int r = 0; r < kRegs; r++) __stcs(p + off0(r), v[r]);
+            continue;
+        }
         if (PH != PH_NONE && !FUSED) apply_phase(L0t(), cbase, g0, g1, g2, g3);
         // Final layout: L1 after an exchange, L0 for <C> (the cut
         // decomposition is per L0 slot) and for fused passes (their second

@@ -343,14 +343,18 @@ def test_state_diff_matches_host(ctx):
     assert d["l2_b"] == pytest.approx(np.linalg.norm(b), rel=1e-12)
 
 
-def test_config2_n30_p5_full_state(ctx, fq):
+@pytest.mark.parametrize("kind", ["int", "fp"])
+def test_config2_n30_p5_full_state(ctx, fq, kind):
     """Benchmark config 2 (K_30, integer weights 1..10, p=5, C=12) at full
-    size: the fused engine against the reference schedule (cost sweep, RX
-    chunks of C=12, block swaps) on every one of the 2^30 amplitudes, in one
-    qubit order, compared on the device (1e-12 of max|psi| and relative L2)."""
+    size, and the same with FP64 weights (G(30, 0.5)): the fused engine
+    against the reference schedule (cost sweep, RX chunks of C=12, block
+    swaps) on every one of the 2^30 amplitudes, in one qubit order,
+    compared on the device (1e-12 of max|psi| and relative L2).  At N=30 the
+    engine's layer-0 pass runs on paired strided tiles with the lane-bit
+    qubit, alternating its exchange direction from tile to tile."""
     n, P, C = 30, 5, 12
     rng = np.random.default_rng(30)
-    W = complete_int(n, rng)
+    W = complete_int(n, rng) if kind == "int" else gnp_fp(n, rng)
     g, b = angles(rng, P)
     a, r, ph = ctx.state(n), ctx.state(n), ctx.state(n)
     try:
