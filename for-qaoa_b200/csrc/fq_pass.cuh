@@ -280,6 +280,13 @@ __device__ __forceinline__ int pbase(int tid) {
     return b;
 }
 
+// Registers from layout LF to LT through buf.  Each thread writes its own
+// LF slots and, after the barrier, reads its own LT slots.  wait_readers
+// adds a barrier before the writes, which only a change of layout needs:
+// an exchange that writes the layout the thread last read (the previous
+// exchange's LT, with no partner reads since, or those behind
+// exchange_lane's warp barrier) writes slots that no other thread reads
+// until the next barrier, and skips it.
 template <int LF, int LT, bool PAIR = false, bool PAD = true>
 __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int tid,
                                          bool wait_readers = true, int grp = 0) {
@@ -822,7 +829,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             if (SC == SC_L021) {
                 exchange<0, 2, PAIR>(v, buf, tid, !(first && skip_lead), grp);
                 rx_regs<G>(v, m_lo, gx, A.c, A.s);
-                exchange<2, 1, PAIR>(v, buf, tid, true, grp);
+                exchange<2, 1, PAIR>(v, buf, tid, false, grp);
             } else if (SC == SC_L01) {
                 if (GM2 == GM_NONE && lo_lane >= 0)
                     exchange_lane<0, 1, G, PAIR>(v, buf, tid, !(first && skip_lead), grp, lo_lane, gx,
@@ -873,11 +880,11 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
                     // as in L0.
                     if (lo_lane >= 0) rx_lane<G2>(v, lo_lane, A.gx2, A.c, A.s);
                     if (SC == SC_L021) {
-                        exchange<1, 2, PAIR>(v, buf, tid, true, grp);
+                        exchange<1, 2, PAIR>(v, buf, tid, false, grp);
                         rx_regs<G2>(v, m_lo, A.gx2, A.c, A.s);
-                        exchange<2, 0, PAIR>(v, buf, tid, true, grp);
+                        exchange<2, 0, PAIR>(v, buf, tid, false, grp);
                     } else {
-                        exchange<1, 0, PAIR>(v, buf, tid, true, grp);
+                        exchange<1, 0, PAIR>(v, buf, tid, false, grp);
                     }
                     if (CPF) {
                         const i64 U2 = U + gridDim.x;
@@ -901,7 +908,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
                     rx_regs<G2>(v, m_hi, A.gx2, A.c, A.s);
                 }
             } else if (SC != SC_L0 && LAY == 0) {
-                exchange<1, 0, PAIR>(v, buf, tid, true, grp);
+                exchange<1, 0, PAIR>(v, buf, tid, false, grp);
             }
         }
         // The cut constants again for the outputs that need them (read back

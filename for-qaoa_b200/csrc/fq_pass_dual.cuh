@@ -283,23 +283,29 @@ __global__ void __launch_bounds__(kPassThreads, 1)
             // The reverse sweep's first pass, back to L0.
             if (SC != SC_L0) rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
             if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
+            // No leading barriers (see exchange): each thread writes the v
+            // slots it has just read, and the w slots were last read in the
+            // previous tile, before this tile's first barrier.
             if (SC == SC_L021) {
-                exchange_dual<1, 2>(v, w, buf, xt, true);
+                exchange_dual<1, 2>(v, w, buf, xt, false);
                 rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
-                exchange_dual<2, 0>(v, w, buf, xt, true);
+                exchange_dual<2, 0>(v, w, buf, xt, false);
             } else if (SC == SC_L01) {
-                exchange_dual<1, 0>(v, w, buf, xt, true);
+                exchange_dual<1, 0>(v, w, buf, xt, false);
             }
             rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
         } else {
         rx_regs_dual<GM>(v, w, m_hi, g, f2, sc, accb);
         if (lo_lane >= 0) rx_lane_dual<GM>(v, w, lo_lane, g, f2, sc, accb);
+        // A fused pass's previous tile ended by reading the thread's own L0
+        // slots, which this exchange writes: no leading barrier (see
+        // exchange); other passes ended in L1 and need it.
         if (SC == SC_L021) {
-            exchange_dual<0, 2>(v, w, buf, xt, true);
+            exchange_dual<0, 2>(v, w, buf, xt, !FUSED);
             rx_regs_dual<GM>(v, w, m_lo, g, f2, sc, accb);
-            exchange_dual<2, 1>(v, w, buf, xt, true);
+            exchange_dual<2, 1>(v, w, buf, xt, false);
         } else if (SC == SC_L01) {
-            exchange_dual<0, 1>(v, w, buf, xt, true);
+            exchange_dual<0, 1>(v, w, buf, xt, !FUSED);
         }
         if (SC != SC_L0) rx_regs_dual<GM>(v, w, m_mid, g, f2, sc, accb);
         if constexpr (PHI) {
@@ -376,11 +382,11 @@ __global__ void __launch_bounds__(kPassThreads, 1)
                 if (SC != SC_L0) rx_regs_dual<GM2>(v, w, m_mid, g2x, f2b, sc2, accb2);
                 if (lo_lane >= 0) rx_lane_dual<GM2>(v, w, lo_lane, g2x, f2b, sc2, accb2);
                 if (SC == SC_L021) {
-                    exchange_dual<1, 2>(v, w, buf, xt, true);
+                    exchange_dual<1, 2>(v, w, buf, xt, false);
                     rx_regs_dual<GM2>(v, w, m_lo, g2x, f2b, sc2, accb2);
-                    exchange_dual<2, 0>(v, w, buf, xt, true);
+                    exchange_dual<2, 0>(v, w, buf, xt, false);
                 } else if (SC == SC_L01) {
-                    exchange_dual<1, 0>(v, w, buf, xt, true);
+                    exchange_dual<1, 0>(v, w, buf, xt, false);
                 }
                 if (CPF) {
                     // Each thread's L0 slots are its own until the next
