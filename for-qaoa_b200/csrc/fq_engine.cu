@@ -432,13 +432,17 @@ static int tile_cut_tables(fq_ctx* ctx, const GraphPrep& g, int N,
         ctx->tcut_bytes = need;
     }
     const int grid = (int)std::min<i64>((ntiles + 7) / 8, (i64)ctx->num_sms * 4);
+    // The attribute is the same for every N: contexts on other threads (the
+    // server's lanes) set it concurrently, and a launch needing more than
+    // another thread's smaller setting would fail.
     const size_t smem = g.integer ? tcut_smem_bytes<int>(N) : tcut_smem_bytes<double>(N);
     if (g.integer)
         FQ_CUDA(cudaFuncSetAttribute(k_tile_cuts<int>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+                                     (int)tcut_smem_bytes<int>(kMaxQubits)));
     else
         FQ_CUDA(cudaFuncSetAttribute(k_tile_cuts<double>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tcut_smem_bytes<double>(kMaxQubits)));
     TcutGeoms G;
     memset(&G, 0, sizeof(G));
     for (size_t i = 0; i < plan.size(); i++) {
