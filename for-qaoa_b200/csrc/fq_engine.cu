@@ -431,7 +431,7 @@ static int tile_cut_tables(fq_ctx* ctx, const GraphPrep& g, int N,
         }
         ctx->tcut_bytes = need;
     }
-    const int grid = (int)std::min<i64>((ntiles + 7) / 8, (i64)ctx->num_sms * 4);
+    const int grid = (int)std::min<i64>((ntiles + 3) / 4, (i64)ctx->num_sms * 8);
     // The attribute is the same for every N: contexts on other threads (the
     // server's lanes) set it concurrently, and a launch needing more than
     // another thread's smaller setting would fail.

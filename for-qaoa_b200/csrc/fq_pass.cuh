@@ -533,23 +533,26 @@ struct CutTables {
         }
     }
 
-    // K and e_u of the tile at `base` into out (one warp): tile()'s two
-    // warps' work in the same order, so the values are the same.
-    __device__ void tile_warp(WT* out, i64 base, int nF, int l, int a, int lane) const {
+    // K (role 0) or e_u (role 1) of the tile at `base` into out (one warp):
+    // tile()'s warp 0 or warp 1 work in the same order, so the values are
+    // the same.
+    __device__ void tile_part(WT* out, i64 base, int nF, int l, int a, int lane,
+                              int role) const {
         const int zi = lane < nF ? (int)((base >> fixed_phys(lane, l, a)) & 1) : 0;
         const unsigned F = __ballot_sync(0xffffffffu, zi);
-        WT h = 0;
-        if (lane < nF) {
-            if (zi) h = Dm[lane];
-            const WT* row = wf + lane * kWfStride;
+        if (role == 0) {
+            WT h = 0;
+            if (lane < nF) {
+                if (zi) h = Dm[lane];
+                const WT* row = wf + lane * kWfStride;
 #pragma unroll
-            for (int j = 1; j < kMaxFixed; j++)
-                if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi)) h += row[j];
-        }
+                for (int j = 1; j < kMaxFixed; j++)
+                    if (j > lane && j < nF && (((F >> j) & 1u) != (unsigned)zi)) h += row[j];
+            }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
-        if (lane == 0) out[0] = h;
-        if (lane < kTileBits) {
+            for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+            if (lane == 0) out[0] = h;
+        } else if (lane < kTileBits) {
             WT e = Ru[lane];
             const WT* row = wu + lane * kWfStride;
 #pragma unroll
@@ -581,8 +584,8 @@ struct CutTables {
 // picks one) for the tile passes to read instead of computing them per
 // tile: out[y * ntiles * kTcutStride + T * kTcutStride] = K, then
 // e_0..e_11 (CutTables::tile).  256 threads set up the tables, then each
-// warp takes tiles.  Shared memory: the N*N weights, rounded up to 16
-// bytes, then PassSmem<WT>.
+// pair of warps takes tiles, K on one, the e_u on the other.  Shared
+// memory: the N*N weights, rounded up to 16 bytes, then PassSmem<WT>.
 constexpr int kTcutStride = 16;
 struct TcutGeoms {
     int l[4], a[4];
@@ -605,10 +608,10 @@ __global__ void __launch_bounds__(kPassThreads) k_tile_cuts(const WT* w, int N, 
     ct.template setup<false>(sw, N, l, a, threadIdx.x, 0.0);
     __syncthreads();
     const int nF = N - kTileBits, nmid = a - l, lane = threadIdx.x & 31;
-    const int wpb = kPassThreads / 32;
-    for (i64 T = (i64)blockIdx.x * wpb + (threadIdx.x >> 5); T < ntiles; T += (i64)gridDim.x * wpb) {
+    const int role = (threadIdx.x >> 5) & 1, tpb = kPassThreads / 64;  // tiles per block and round
+    for (i64 T = (i64)blockIdx.x * tpb + (threadIdx.x >> 6); T < ntiles; T += (i64)gridDim.x * tpb) {
         const i64 base = ((T & ((1ll << nmid) - 1)) << l) | ((T >> nmid) << (a + kTileBits - l));
-        ct.tile_warp(out + T * kTcutStride, base, nF, l, a, lane);
+        ct.tile_part(out + T * kTcutStride, base, nF, l, a, lane, role);
     }
 }
 
