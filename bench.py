@@ -13,10 +13,13 @@ Also reported on the same JSON line:
   e2e          the same circuit through the public C ABI with host inputs:
                the graph is uploaded from pinned host memory every step and
                <C> is read back to the host every step;
-  roofline     the dominant kernel (the strided tile pass, k_pass_tma):
-               algorithmic bytes per launch / average launch time (CUDA
-               events on the library's stream), against the measured HBM copy
-               bandwidth; per_layer gives the same over every pass of a layer;
+  roofline     the dominant kernel kind (the one with the largest share of
+               device time: at N=30 the fused passes and the mixer passes
+               take nearly equal shares, so either can lead): algorithmic
+               bytes per launch / average launch time (CUDA events on the
+               library's stream), against the measured HBM copy bandwidth;
+               per_kind gives every kind, per_layer the same over every pass
+               of a layer;
   cpu_baseline the oracle (plain FP64 OpenMP restatement of the reference's
                algorithm) timed on the host cores on one whole N=30 layer of
                a full 16 GiB host state, beside the estimate from timed
