@@ -573,17 +573,18 @@ def eval_bytes(ctx, n, P, cache):
 def serving_ceiling(seq, peak_gbs, sms):
     """Best speed-up over sequential calls this stream allows: every request
     at least its HBM roofline time (algorithmic bytes / measured copy
-    bandwidth; requests share one HBM), a one-CTA request (N <= 12) at least
-    its sequential time spread over every SM.  ceiling = sum of sequential
-    times / sum of those bounds."""
+    bandwidth; requests share one HBM), a request held in shared memory
+    (N <= 15: one CTA up to 12 qubits, a cluster of 2^(N-12) CTAs above) at
+    least its sequential time times its share of the SMs.  ceiling = sum of
+    sequential times / sum of those bounds."""
     import forqaoa
     cache = {}
     t_seq = t_bound = 0.0
     with forqaoa.Context(0) as ctx:
         for r in seq:
             t_seq += r["latency"]
-            if r["N"] <= 12:
-                t_bound += r["latency"] / sms
+            if r["N"] <= forqaoa.SMALL_MAX_QUBITS:
+                t_bound += r["latency"] * (1 << max(0, r["N"] - 12)) / sms
             else:
                 t_bound += eval_bytes(ctx, r["N"], r["P"], cache) / (peak_gbs * 1e9)
     return t_seq / t_bound, t_seq, t_bound
@@ -609,7 +610,8 @@ def serving_leg(args):
     out["ceiling_speedup_vs_sequential"] = ceil
     out["ceiling_note"] = ("sum of sequential times %.1f s / sum of per-request bounds %.1f s "
                            "(HBM roofline of each request's algorithmic bytes at %.0f GB/s; "
-                           "one-CTA requests: sequential time / 148 SMs)" % (t_seq, t_bound, peak))
+                           "shared-memory requests, N <= 15: sequential time x their CTAs / "
+                           "148 SMs)" % (t_seq, t_bound, peak))
     out["stream"] = {"sessions": len(sessions), "steps": steps, "n": [10, 28], "p": [1, 8],
                      "graph": "G(N,0.5), integer weights 1..10", "seed": 5,
                      "arrivals": "Poisson, mean gap 1 ms (arrivals outpace the device: "
@@ -635,8 +637,8 @@ def serving_leg(args):
     # which 1 ms-spaced arrivals offer work (a session of small requests ends
     # in a few milliseconds).
     out["by_size"] = {}
-    for lo, hi, n_req, lanes in ((10, 12, 4000, args.serve_lanes), (13, 20, 2000, 16),
-                                 (21, 28, 200, args.serve_lanes)):
+    for lo, hi, n_req, lanes in ((10, 12, 4000, args.serve_lanes), (13, 15, 2000, args.serve_lanes),
+                                 (16, 20, 2000, 16), (21, 28, 200, args.serve_lanes)):
         sess, steps = ss.make_stream(n_req, seed=lo, n_min=lo, n_max=hi, mean_gap_ms=0.01)
         sv, w, _ = ss.run_native("served", sess, steps, lanes=lanes)
         sq, wq, _ = ss.run_native("sequential", sess, steps)

@@ -67,8 +67,9 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
 int grad_collect(fq_ctx* ctx, int N, int P, double* energy, double* grad_gamma,
                  double* grad_beta);
 
-// One CTA per job of k_small_jobs (fq_small.cuh); nmax = largest N.
-
-int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream);
+// k_small_jobs (fq_small.cuh) over jobs ordered by size class
+// (small_class): counts[c] jobs of class c, one launch per class present;
+// nmax0 = the largest N of class 0.
+int launch_small_jobs(const SmallJob* jobs, const int* counts, int nmax0, cudaStream_t stream);
 
 }  // namespace fq

@@ -47,11 +47,47 @@ __global__ void k_reduce_grad(const double* part, int grid, const GradSums S, do
     if (threadIdx.x == 0) out[d] = sh[0];
 }
 
-int launch_small_jobs(const SmallJob* jobs, int njobs, int nmax, cudaStream_t stream) {
-    FQ_CUDA(cudaFuncSetAttribute(k_small_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// n jobs of one size class: CB = 0 (N <= 12, one CTA each, nl = the
+// largest N) or CB = N - 12 (a cluster of 2^CB CTAs each, nl = 12).
+template <int CB>
+static int launch_small_class(const SmallJob* jobs, int n, int nl, cudaStream_t stream) {
+    auto fn = k_small_jobs<CB>;
+    FQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)small_smem_bytes(kSmallMaxQubits)));
-    k_small_jobs<<<njobs, kSmallThreads, small_smem_bytes(nmax), stream>>>(jobs, njobs);
-    FQ_CUDA(cudaGetLastError());
+    if (CB == 0) {
+        fn<<<n, kSmallThreads, small_smem_bytes(nl), stream>>>(jobs, n);
+        FQ_CUDA(cudaGetLastError());
+        return FQ_OK;
+    }
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)n << CB);
+    cfg.blockDim = dim3(kSmallThreads);
+    cfg.dynamicSmemBytes = small_smem_bytes(kSmallMaxQubits);
+    cfg.stream = stream;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = 1u << CB;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    FQ_CUDA(cudaLaunchKernelEx(&cfg, fn, jobs, n));
+    return FQ_OK;
+}
+
+int launch_small_jobs(const SmallJob* jobs, const int* counts, int nmax0, cudaStream_t stream) {
+    int off = 0;
+    for (int c = 0; c <= kSmallJobMaxQubits - kSmallMaxQubits; c++) {
+        if (counts[c] == 0) continue;
+        switch (c) {
+            case 0: FQ_TRY(launch_small_class<0>(jobs, counts[0], nmax0, stream)); break;
+            case 1: FQ_TRY(launch_small_class<1>(jobs + off, counts[1], 12, stream)); break;
+            case 2: FQ_TRY(launch_small_class<2>(jobs + off, counts[2], 12, stream)); break;
+            default: FQ_TRY(launch_small_class<3>(jobs + off, counts[3], 12, stream)); break;
+        }
+        off += counts[c];
+    }
     return FQ_OK;
 }
 
@@ -73,7 +109,7 @@ static int run_small_jobs(fq_ctx* ctx, const SmallHostJob* jobs, int njobs, int 
     int nmax = 1, outw = 0;
     for (int i = 0; i < njobs; i++) {
         need += sizeof(double) * (jobs[i].N * jobs[i].N + 2 * jobs[i].P);
-        nmax = std::max(nmax, jobs[i].N);
+        if (small_class(jobs[i].N) == 0) nmax = std::max(nmax, jobs[i].N);  // class 0's largest
         outw += 1 + 2 * jobs[i].P;
     }
     FQ_CHECK(need <= ctx->h_stage_bytes && need <= kScratchBytes, FQ_ERR_INVALID,
@@ -112,7 +148,12 @@ static int run_small_jobs(fq_ctx* ctx, const SmallHostJob* jobs, int njobs, int 
     FQ_CUDA(cudaMemcpyAsync(ctx->d_scratch, h, need, cudaMemcpyHostToDevice, ctx->stream));
     FQ_CUDA(cudaEventRecord(ctx->stage_evt, ctx->stream));
     const int tok = prof_begin(ctx);
-    FQ_TRY(launch_small_jobs(reinterpret_cast<const SmallJob*>(ctx->d_scratch), njobs, nmax,
+    int counts[kSmallClasses] = {};
+    for (int i = 0; i < njobs; i++) counts[small_class(jobs[i].N)]++;
+    for (int i = 1; i < njobs; i++)
+        FQ_CHECK(small_class(jobs[i].N) >= small_class(jobs[i - 1].N), FQ_ERR_INVALID,
+                 "small jobs must come ordered by size class");
+    FQ_TRY(launch_small_jobs(reinterpret_cast<const SmallJob*>(ctx->d_scratch), counts, nmax,
                              ctx->stream));
     prof_end(ctx, tok, FQ_KIND_OTHER, 0.0);
     ctx->launches++;
@@ -312,7 +353,7 @@ int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P, cons
              kMaxQubits);
     FQ_TRY(check_angles(P, gammas, betas));
     FQ_CHECK(energy && grad_gamma && grad_beta, FQ_ERR_INVALID, "null output");
-    if (N <= kSmallMaxQubits) {
+    if (N <= kSmallJobMaxQubits) {
         FQ_CHECK(1 + 2 * P <= kResultWords, FQ_ERR_INVALID, "P=%d too large", P);
         GraphPrep g;
         FQ_TRY(prep_graph(graph, N, g));

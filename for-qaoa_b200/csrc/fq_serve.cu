@@ -4,16 +4,18 @@
 // GPU; a scheduler thread runs the small-instance batches and every lane has
 // a thread of its own, so the ~30 kernel launches of a larger request are
 // issued by its lane's thread, in parallel with the other lanes':
-//   - small instances (N <= 12) are packed one per CTA into launches of
-//     k_small_jobs (the whole instance in shared memory); two batches can be
-//     in flight on their own streams, and a batch takes every small request
-//     queued when it launches (up to its capacity);
+//   - small instances (N <= 15) are packed into launches of k_small_jobs,
+//     the whole instance in shared memory: one CTA each up to 12 qubits, a
+//     cluster of 2^(N-12) CTAs above (distributed shared memory), one launch
+//     per size class; two batches can be in flight on their own streams,
+//     and a batch takes every small request queued when it launches (up to
+//     its capacity);
 //   - larger instances run on lanes (an fq_ctx each: its own stream and
 //     scratch), so independent requests overlap; a free lane takes the
 //     oldest queued request whose session is idle and whose buffers are
 //     resident or fit the HBM budget.
 // A session is a sequence of steps on one graph (an optimiser loop).  For
-// N >= 13 its state and costate buffers (2 x 16 x 2^N bytes) stay resident
+// N >= 16 its state and costate buffers (2 x 16 x 2^N bytes) stay resident
 // across steps in a pool owned by the server and are released when the
 // session is closed or, least recently used first, when another session
 // needs the room.  Cut values are recomputed on the fly from the weights, so
@@ -173,15 +175,23 @@ struct fq_server {
         cv_done.notify_all();
     }
 
-    // ---- small instances (one CTA each) -------------------------------------
+    // ---- small instances (one CTA each, or one cluster of CTAs) --------------
     static size_t job_bytes(const Req& r) {
         return sizeof(SmallJob) + sizeof(double) * (r.N * r.N + 2 * r.P);
     }
 
     int launch_batch(Batch& B) {
         const int nj = (int)B.reqs.size();
-        int nmax = 1;
-        for (auto& r : B.reqs) nmax = std::max(nmax, r.N);
+        // One launch per size class (one CTA, clusters of 2, 4, 8 CTAs):
+        // the batch in class order.
+        std::stable_sort(B.reqs.begin(), B.reqs.end(), [](const Req& a, const Req& b) {
+            return small_class(a.N) < small_class(b.N);
+        });
+        int nmax = 1, counts[kSmallClasses] = {};
+        for (auto& r : B.reqs) {
+            counts[small_class(r.N)]++;
+            if (small_class(r.N) == 0) nmax = std::max(nmax, r.N);
+        }
         SmallJob* hj = reinterpret_cast<SmallJob*>(B.h_in);
         double* hd = reinterpret_cast<double*>(B.h_in + sizeof(SmallJob) * nj);
         const double* dd = reinterpret_cast<const double*>(B.d_in + sizeof(SmallJob) * nj);
@@ -212,7 +222,7 @@ struct fq_server {
         }
         const size_t need = sizeof(SmallJob) * nj + sizeof(double) * off;
         FQ_CUDA(cudaMemcpyAsync(B.d_in, B.h_in, need, cudaMemcpyHostToDevice, B.st));
-        FQ_TRY(launch_small_jobs(reinterpret_cast<const SmallJob*>(B.d_in), nj, nmax, B.st));
+        FQ_TRY(launch_small_jobs(reinterpret_cast<const SmallJob*>(B.d_in), counts, nmax, B.st));
         FQ_CUDA(cudaMemcpyAsync(B.h_out, B.d_out, sizeof(double) * o, cudaMemcpyDeviceToHost,
                                 B.st));
         FQ_CUDA(cudaEventRecord(B.done, B.st));
@@ -582,7 +592,7 @@ int fq_server_submit(fq_server* S, const fq_request* q, uint64_t* ticket) {
     r.P = q->P;
     r.gammas.assign(q->gammas, q->gammas + q->P);
     r.betas.assign(q->betas, q->betas + q->P);
-    const bool small = q->N <= kSmallMaxQubits;
+    const bool small = q->N <= kSmallJobMaxQubits;
     if (small)
         r.w = g.wd;
     else

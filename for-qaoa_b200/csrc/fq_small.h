@@ -1,12 +1,14 @@
 // fq_small.h -- job descriptor of k_small_jobs (fq_small.cuh): one whole
-// QAOA instance of up to 12 qubits per CTA.
+// QAOA instance of up to 12 qubits per CTA, of 13..15 qubits per cluster of
+// 2^(N-12) CTAs.
 #pragma once
 
 #include "fq_common.cuh"
 
 namespace fq {
 
-constexpr int kSmallMaxQubits = 12;
+constexpr int kSmallMaxQubits = 12;     // qubits held by one CTA
+constexpr int kSmallJobMaxQubits = 15;  // qubits of a job (a cluster of up to 8 CTAs)
 constexpr int kSmallThreads = 256;
 
 enum { SJ_ENERGY = 1, SJ_GRAD = 2, SJ_STATE = 4 };
@@ -20,10 +22,20 @@ struct SmallJob {
     double2* state;        // final forward state (SJ_STATE), 2^N (device)
 };
 
-__host__ __device__ inline size_t small_smem_bytes(int nmax) {
-    const size_t n = (size_t)1 << nmax;
+// Shared memory of a CTA holding 2^nl amplitudes: psi, lambda, the cut
+// values, the weights of a job of up to kSmallJobMaxQubits qubits, the
+// block-sum scratch and the cluster's exchange words.
+// Size class of an N-qubit job: 0 for one CTA (N <= 12), else the log2 of
+// its cluster's CTAs.
+constexpr int kSmallClasses = kSmallJobMaxQubits - kSmallMaxQubits + 1;
+__host__ __device__ inline int small_class(int N) {
+    return N <= kSmallMaxQubits ? 0 : N - kSmallMaxQubits;
+}
+
+__host__ __device__ inline size_t small_smem_bytes(int nl) {
+    const size_t n = (size_t)1 << nl;
     return 2 * n * sizeof(double2) + n * sizeof(double) +
-           sizeof(double) * (kSmallMaxQubits * kSmallMaxQubits + kSmallThreads);
+           sizeof(double) * (kSmallJobMaxQubits * kSmallJobMaxQubits + kSmallThreads + 8);
 }
 
 }  // namespace fq

@@ -152,7 +152,7 @@ void run_sequential(std::vector<Sess>& ss, int steps, bool reuse, std::vector<Re
     for (int i : order) {
         Sess& s = ss[i];
         void *sv = nullptr, *cs = nullptr;
-        if (reuse && s.N > 12) {
+        if (reuse && s.N > FQ_SMALL_MAX_QUBITS) {
             if ((st = fq_state_alloc(ctx, s.N, &sv)) || (st = fq_state_alloc(ctx, s.N, &cs)))
                 die("fq_state_alloc", st);
         }
@@ -160,9 +160,10 @@ void run_sequential(std::vector<Sess>& ss, int steps, bool reuse, std::vector<Re
         for (int k = 0; k < steps; k++) {
             double e;
             const double t1 = now_s();
-            // A plain call allocates its state and costate (N > 12) and frees
-            // them afterwards, inside the timed call.
-            const bool own = !reuse && s.N > 12;
+            // A plain call allocates its state and costate (above
+            // FQ_SMALL_MAX_QUBITS) and frees them afterwards, inside the
+            // timed call.
+            const bool own = !reuse && s.N > FQ_SMALL_MAX_QUBITS;
             if (own && ((st = fq_state_alloc(ctx, s.N, &sv)) || (st = fq_state_alloc(ctx, s.N, &cs))))
                 die("fq_state_alloc", st);
             st = fq_qaoa_energy_grad(ctx, sv, cs, s.N, s.P, s.graph.data(), s.g.data(),

@@ -14,6 +14,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libforqaoa.so")
+# FQ_SMALL_MAX_QUBITS of include/forqaoa.h: energy+gradient instances up to
+# this size run wholly in shared memory and need no state buffers.
+SMALL_MAX_QUBITS = 15
 
 OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_BUSY = range(7)
 
@@ -303,13 +306,13 @@ class Context:
     def energy_grad(self, n, graph, gammas, betas, sv=None, costate=None):
         """(<C>, dE/dgamma[P], dE/dbeta[P]) by the adjoint method.  sv and
         costate are DeviceState workspaces of n qubits (allocated here when
-        omitted and n > 12)."""
+        omitted and n > SMALL_MAX_QUBITS)."""
         g = _f64(graph)
         ga, be = _f64(gammas), _f64(betas)
         P = len(ga)
         e, gg, gb = np.zeros(1), np.zeros(P), np.zeros(P)
         own = []
-        if n > 12:
+        if n > SMALL_MAX_QUBITS:
             if sv is None:
                 sv = DeviceState(self, n)
                 own.append(sv)

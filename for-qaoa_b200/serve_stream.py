@@ -27,7 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 if HERE not in sys.path:
     sys.path.insert(0, HERE)
 
-BUCKETS = ((2, 12, "one CTA each (N<=12)"), (13, 20, "lanes, N 13..20"),
+BUCKETS = ((2, 15, "one CTA or cluster each (N<=15)"), (16, 20, "lanes, N 16..20"),
            (21, 33, "lanes, N 21..28"))
 
 
@@ -109,7 +109,7 @@ def run_sequential(fq, sessions, steps, device=0, reuse=True):
         for s in sorted(sessions, key=lambda s: s["arrival"]):
             n = s["N"]
             sv = cs = None
-            if n > 12 and reuse:
+            if n > fq.SMALL_MAX_QUBITS and reuse:
                 sv, cs = ctx.state(n), ctx.state(n)
             g, b = s["gammas"].copy(), s["betas"].copy()
             for k in range(steps):

@@ -166,9 +166,11 @@ int fq_qaoa_forward(fq_ctx* ctx, void* sv, int N, int P, const double* graph_upp
  * through the exact inverse of each layer (no stored intermediate states):
  *   dE/dbeta_k = Im <lambda|sum_q X_q|psi>,  dE/dgamma_k = -Im <lambda|S|psi>.
  * sv and costate are device workspaces of 2^N amplitudes each (contents
- * unspecified on return; unused, may be NULL, for N <= 12, where the whole
- * instance runs in one CTA's shared memory).  Writes *energy, grad_gamma[P],
+ * unspecified on return; unused, may be NULL, for N <= FQ_SMALL_MAX_QUBITS,
+ * where the whole instance runs in shared memory: one CTA's up to 12
+ * qubits, a cluster of 2^(N-12) CTAs above).  Writes *energy, grad_gamma[P],
  * grad_beta[P] (host) and synchronises. */
+#define FQ_SMALL_MAX_QUBITS 15
 int fq_qaoa_energy_grad(fq_ctx* ctx, void* sv, void* costate, int N, int P,
                         const double* graph_upper, const double* gammas, const double* betas,
                         double* energy, double* grad_gamma, double* grad_beta);
@@ -206,10 +208,10 @@ int fq_reference_label_map(int N, int C, int P, int* label_map);
 /* ---- serving -------------------------------------------------------------
  * A server admits energy+gradient requests (fq_qaoa_energy_grad's
  * computation) and runs them with continuous batching on one device:
- * requests with N <= 12 are packed one per CTA into batched launches,
- * larger ones overlap on `lanes` independent streams.  Requests of one
- * session (an optimiser loop on one graph) run in submission order and, for
- * N >= 13, keep their state and costate buffers (2 x 16 x 2^N bytes)
+ * requests with N <= FQ_SMALL_MAX_QUBITS are packed one per CTA (N <= 12)
+ * or one per cluster of CTAs into batched launches, larger ones overlap on
+ * `lanes` independent streams.  Requests of one session (an optimiser loop
+ * on one graph) run in submission order and, for larger N, keep their state and costate buffers (2 x 16 x 2^N bytes)
  * resident between steps; resident buffers stay within hbm_budget_bytes,
  * idle sessions being released least recently used first.  No counterpart
  * in the reference, whose CLI runs one circuit per process

@@ -112,8 +112,9 @@ print(json.dumps(out))
 
 
 # The pass that completes a layer alternates between the contiguous pass and
-# the last strided pass, whose tile schedule is L0 (N 13..16, 24), L01
-# (17..21, 25..30) or L021 (22, 23); P = 1 has no fused pass; "huge" weights
+# the last strided pass, whose tile schedule is L0 (N 16, 24), L01
+# (17..21, 25..30) or L021 (22, 23) (up to 15 qubits the whole instance runs
+# in shared memory, one CTA or one cluster); P = 1 has no fused pass; "huge" weights
 # take one phase table per layer, FP64 weights with a large sum ("wide" plus
 # a quarter) one sincos per amplitude.
 @pytest.mark.parametrize("fuse", ["1", "0"])

@@ -17,6 +17,8 @@ class _R:
 
 
 class FakeFQ:
+    SMALL_MAX_QUBITS = 15  # the library's FQ_SMALL_MAX_QUBITS
+
     def __init__(self, oracle, seed=0):
         self.rng = np.random.default_rng(seed)
         self.submitted = []
