@@ -53,8 +53,11 @@ def test_mix_matches_alone(fq, ctx, oracle):
 
 
 def test_small_requests_share_launches(fq, ctx):
+    """Requests of 2..15 qubits (one CTA up to 12, a cluster of 2, 4 or 8
+    CTAs above) are batched, one launch per size class and batch."""
     rng = np.random.default_rng(11)
-    reqs = [(i, *make_request(rng, int(rng.integers(2, 13)), int(rng.integers(1, 9))))
+    reqs = [(i, *make_request(rng, int(rng.integers(2, fq.SMALL_MAX_QUBITS + 1)),
+                              int(rng.integers(1, 9))))
             for i in range(600)]
     with fq.Server(0, 1e9, lanes=1) as srv:
         tickets = {srv.submit(i, W, g, b): i for i, W, g, b in reqs}
