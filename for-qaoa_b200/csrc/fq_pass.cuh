@@ -860,10 +860,13 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             continue;
         }
         if (PH != PH_NONE && !FUSED) apply_phase(L0t(), cbase, g0, g1, g2, g3);
-        // Final layout: L1 after an exchange, L0 for <C> (the cut
-        // decomposition is per L0 slot) and for fused passes (their second
-        // rounds run back from L1 to L0).
-        constexpr int LAY = (GM != GM_NONE && SC != SC_L0 && EX == EX_NONE && !FUSED) ? 1 : 0;
+        // Final layout: L1 after an exchange (<C> then takes the cut
+        // constants of L1), L0 for the costate and the diagonal (written at
+        // L0 addresses) and for fused passes (their second rounds run back
+        // from L1 to L0).
+        constexpr int LAY =
+            (GM != GM_NONE && SC != SC_L0 && (EX == EX_NONE || EX == EX_ENERGY) && !FUSED) ? 1
+                                                                                          : 0;
         if (GM != GM_NONE) {
             rx_rounds(std::integral_constant<int, GM>(), A.gx, true);
             if (FUSED) {
@@ -916,11 +919,12 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
         }
         // The cut constants again for the outputs that need them (read back
         // instead of held in registers through the rounds above).
-        if (EX != EX_NONE) ct.consts(kp, tid, cbase, g0, g1, g2, g3);
+        if (EX != EX_NONE) ct.template consts<LAY>(kp, tid, cbase, g0, g1, g2, g3);
+        const WT* const crg = ct.creg + 16 * LAY;
         if (EX == EX_DIAG) {
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 __stcs(A.diag + base + thr_off + off0(r), (double)cr);
             }
@@ -929,7 +933,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
             double ts = 0;
 #pragma unroll
             for (int r = 0; r < kRegs; r++) {
-                const WT cr = cbase + ct.creg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
+                const WT cr = cbase + crg[r] + ((r & 1) ? g0 : WT(0)) + ((r & 2) ? g1 : WT(0)) +
                               ((r & 4) ? g2 : WT(0)) + ((r & 8) ? g3 : WT(0));
                 ts = fma(fma(v[r].x, v[r].x, v[r].y * v[r].y), (double)cr, ts);
                 if (EX == EX_COSTATE) {
