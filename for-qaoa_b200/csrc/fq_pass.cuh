@@ -437,7 +437,9 @@ struct CutTables {
 
     // Fill the tables from the N*N weights sw (shared memory, all threads;
     // the caller synchronises before and after).  QT: also z^creg[r].
-    template <bool QT>
+    // THR: also the per-thread constants (thrc), which the tile-cut table
+    // kernel does not need.
+    template <bool QT, bool THR = true>
     __device__ void setup(const WT* sw, int N, int l, int a, int tid, double gamma) const {
         const int nF = N - kTileBits;
         for (int idx = tid; idx < nF * nF; idx += kPassThreads) {
@@ -472,7 +474,7 @@ struct CutTables {
                 qtab[16 * L + r] = make_double2(cs, sn);
             }
         }
-        for (int L = 0; L < 2; L++) {
+        for (int L = 0; L < (THR ? 2 : 0); L++) {
             const int T = L == 0 ? tid : lay_index<1>(tid, 0);  // slot 0's tile index
             WT athr = 0, f[4] = {0, 0, 0, 0};
             for (int j = 0; j < 8; j++) {
@@ -605,7 +607,7 @@ __global__ void __launch_bounds__(kPassThreads) k_tile_cuts(const WT* w, int N, 
     const CutTables<WT> ct(smraw + ((N * N * sizeof(WT) + 15) & ~(size_t)15));
     for (int i = threadIdx.x; i < N * N; i += kPassThreads) sw[i] = w[i];
     __syncthreads();
-    ct.template setup<false>(sw, N, l, a, threadIdx.x, 0.0);
+    ct.template setup<false, false>(sw, N, l, a, threadIdx.x, 0.0);
     __syncthreads();
     const int nF = N - kTileBits, nmid = a - l, lane = threadIdx.x & 31;
     const int role = (threadIdx.x >> 5) & 1, tpb = kPassThreads / 64;  // tiles per block and round
