@@ -28,6 +28,8 @@ Also reported on the same JSON line:
                chunks of C=12, block swaps) through this library's per-kernel
                entry points, with per-kernel HBM GB/s;
   gradient     <C> and its 2p derivatives (adjoint) for K_26, p=10;
+  config3      the N=32 p=3 circuit on a 3-regular graph with FP64 weights
+               (64 GiB state): layers/s and per-layer HBM fraction;
   serving      a sample of the served request stream (sessions of 20
                energy+gradient steps, N in 10..28, p in 1..8) through the
                server against the same evaluations as sequential calls, plus
@@ -90,6 +92,8 @@ def parse_args(argv=None):
                     help="requests of the served leg's sustainable-rate latency run")
     ap.add_argument("--serve-lanes", type=int, default=4)
     ap.add_argument("--no-grad", action="store_true", help="skip the adjoint-gradient leg")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip the N=32 p=3 (3-regular, FP64 weights) circuit leg")
     return ap.parse_args(argv)
 
 
@@ -511,6 +515,9 @@ def run_ours(args):
     # ---- adjoint gradient of the N=26 p=10 circuit (one GPU)
     if not args.no_grad and d.world == 1:
         line["gradient"] = gradient_leg(ctx, peak)
+    # ---- config 3: N=32 p=3, 3-regular graph with FP64 weights (one GPU)
+    if not args.no_config3 and d.world == 1:
+        line["config3"] = config3_leg(ctx, peak)
     # ---- served energy+gradient stream vs sequential plain calls (one GPU)
     if args.serve_requests > 0 and d.world == 1:
         line["serving"] = serving_leg(args)
@@ -552,6 +559,69 @@ def gradient_leg(ctx, peak, n=26, P=10, reps=5):
         out["kernels"][kind] = {"launches": kn // reps, "ms_per_eval": kms / reps, "gbs": gbs,
                                 "frac": gbs / peak if gbs else None}
     return out
+
+
+def regular3(n, rng):
+    """A random 3-regular graph on n vertices by seeded pairing of 3n
+    half-edges, redrawn while a pairing has a loop or a double edge."""
+    while True:
+        pts = rng.permutation(np.repeat(np.arange(n), 3))
+        edges = set()
+        for i in range(0, 3 * n, 2):
+            u, v = int(min(pts[i], pts[i + 1])), int(max(pts[i], pts[i + 1]))
+            if u == v or (u, v) in edges:
+                break
+            edges.add((u, v))
+        else:
+            return sorted(edges)
+
+
+def config3_leg(ctx, peak, n=32, P=3, reps=3):
+    """Benchmark config 3: N=32 (a 64 GiB state), p=3, a random 3-regular
+    graph (48 edges) with FP64 weights in [0, 1), seeded.  The fused engine
+    at three passes per layer (the contiguous one and two strided passes of
+    10 qubits each over rows of 4 amplitudes); FP64 phases take the product
+    tree where the weights' sum times |gamma| allows it, else one sincos of
+    the reference's argument per amplitude.  layers/s from CUDA events on the
+    library's stream, and the per-layer HBM fraction over every pass."""
+    import torch
+    rng = np.random.default_rng(32)
+    W = np.zeros((n, n))
+    for u, v in regular3(n, rng):
+        W[u, v] = rng.uniform(0.0, 1.0)
+    g, b = rng.uniform(0, np.pi, P), rng.uniform(0, np.pi / 2, P)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = ctx.state(n)
+    try:
+        ctx.qaoa_forward(st, W, g, b, energy=False)  # warm-up
+        ctx.synchronize()
+        ctx.profile_reset()
+        ctx.set_profiling(True)
+        e0.record(stream)
+        for _ in range(reps):
+            ctx.qaoa_forward(st, W, g, b, energy=False)
+        e1.record(stream)
+        ctx.synchronize()
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        energy = ctx.qaoa_forward(st, W, g, b, energy=True)
+    finally:
+        st.free()
+    ms = e0.elapsed_time(e1)
+    kb = sum(v[2] for k, v in prof.items() if k in ("init_pass", "phase_pass", "mixer_pass"))
+    kms = sum(v[0] for k, v in prof.items() if k in ("init_pass", "phase_pass", "mixer_pass"))
+    gbs = kb / (kms / 1000.0) / 1e9 if kms else None
+    return {"workload": f"N={n} p={P}, random 3-regular graph (48 edges), FP64 weights "
+                        "U[0,1), complex128 state (64 GiB), seed 32",
+            "layers_per_s": P * reps / (ms / 1000.0), "ms_per_circuit": ms / reps,
+            "energy": energy,
+            "per_layer": {"gbs": gbs, "frac": gbs / peak if gbs else None,
+                          "sweeps_per_layer": sum(v[1] for k, v in prof.items()
+                                                  if k in ("init_pass", "phase_pass",
+                                                           "mixer_pass")) / (P * reps)},
+            "kernels": {k: {"launches": v[1] // reps, "ms_per_circuit": v[0] / reps}
+                        for k, v in prof.items()}}
 
 
 def eval_bytes(ctx, n, P, cache):

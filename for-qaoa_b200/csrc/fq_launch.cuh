@@ -40,7 +40,11 @@ inline double pass_bytes(int N) {
 // rows).  Measured on B200 at N=30, p=5 (A/B in one call): 59.8-60.1
 // layers/s with every such pass paired, 59.5-59.7 with the strided RX pass
 // on the TMA pipeline instead.
-inline bool pair_ok(const PassArgs& A) { return A.l == 3 && A.a > A.l && A.ntiles >= 2; }
+// Strided tiles with rows of 2, 4 or 8 amplitudes run paired (k_pass PAIR):
+// rows of 16 and more are DRAM-friendly alone.  Rows of 2 and 4 (N = 23,
+// 22, 32) paired: 0.527 against 0.542 ms per N=23 circuit (p=5), 233
+// against 242 ms per N=32 circuit (p=3), A/B in one call.
+inline bool pair_ok(const PassArgs& A) { return A.l >= 1 && A.l <= 3 && A.a > A.l && A.ntiles >= 2; }
 
 template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
           bool PAIR = false>

@@ -643,12 +643,13 @@ __device__ __forceinline__ double2 phase_of(const PassArgs& A, const double2* sm
 // reversed every other layer, the last pass of one layer and the first of
 // the next share a tile geometry, so two sweeps become one.
 //
-// PAIR (strided tiles with 128-byte rows, l = 3): 512 threads, one CTA per
-// SM, as two 256-thread groups that take the two tiles differing only in
-// physical bit 3 (tile numbers 2t and 2t+1) at the same time, each with its
-// own exchange buffer, tile constants and named barrier.  Their loads and
-// stores then meet DRAM as 256-byte rows: per-thread sweeps over 128-byte
-// rows measured 4.1-4.9 TB/s on B200 at N=30, over 256-byte rows 5.6 TB/s.
+// PAIR (strided tiles with rows of 2 to 8 amplitudes, l = 1..3): 512
+// threads, one CTA per SM, as two 256-thread groups that take the two tiles
+// differing only in physical bit l (tile numbers 2t and 2t+1) at the same
+// time, each with its own exchange buffer, tile constants and named
+// barrier.  Their loads and stores then meet DRAM as rows twice as long
+// (256 bytes at l = 3): per-thread sweeps over 128-byte rows measured
+// 4.1-4.9 TB/s on B200 at N=30, over 256-byte rows 5.6 TB/s.
 template <typename WT, int PH, int GM, int EX, bool ST, int SC, int GM2 = GM_NONE,
           bool PAIR = false>
 __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ? 1 : 2)
