@@ -82,3 +82,20 @@ def test_reference_arm_under_torchrun_prints_once():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
     assert len(lines) == 1 and lines[0]["n_gpus"] == 2
+
+
+def test_config3_graph_is_seeded_3_regular():
+    """The config-3 leg's graph: 48 distinct edges on 32 vertices, each vertex
+    of degree 3, the same for the same seed."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import bench
+    e1 = bench.regular3(32, np.random.default_rng(32))
+    e2 = bench.regular3(32, np.random.default_rng(32))
+    assert e1 == e2 and len(e1) == 48 and len(set(e1)) == 48
+    deg = np.zeros(32, dtype=int)
+    for u, v in e1:
+        assert 0 <= u < v < 32
+        deg[u] += 1
+        deg[v] += 1
+    assert (deg == 3).all()
