@@ -103,6 +103,7 @@ int upload_graph(fq_ctx* ctx, const GraphPrep& g, const double* upper) {
     ctx->g_key.assign(upper, upper + nn);
     ctx->g_key.push_back(g.integer ? 1.0 : 0.0);
     ctx->g_n = g.N;
+    ctx->g_version++;
     return FQ_OK;
 }
 

@@ -21,6 +21,8 @@ struct fq_ctx {
     int* d_err = nullptr;         // kernels' error flag (nonzero: a bounded wait gave up)
     void* d_tcut = nullptr;       // per-tile cut constants of the engine's passes (grown on demand)
     size_t tcut_bytes = 0;
+    long long tcut_version = -1;  // g_version the tables were built for (-1: none)
+    int tcut_n = -1;              // and N
     int partial_cap = 0;
     // Pinned host staging (uploads of weights and small tables).
     unsigned char* h_stage = nullptr;
@@ -30,6 +32,7 @@ struct fq_ctx {
     // Graph cache: the last weights uploaded to d_w.
     std::vector<double> g_key;
     int g_n = -1;
+    long long g_version = 0;  // counts uploads: d_w changed
     long long launches = 0;
     // Optional per-kernel timing (fq_ctx_set_profiling): an event pair per
     // launch, resolved when the profile is read.

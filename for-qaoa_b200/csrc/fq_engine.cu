@@ -399,7 +399,8 @@ int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g) {
 }
 
 // Cut constants of every tile of each plan geometry (k_tile_cuts, one
-// launch) in ctx->d_tcut, grown on demand: tabs[i] serves plan[i].  Below
+// launch) in ctx->d_tcut, grown on demand and kept while the weights and N
+// stay the same: tabs[i] serves plan[i].  Below
 // N = 21 (512 tiles) and without the buffer (a failed allocation) tabs
 // stays null and the passes compute the constants per tile, as they do for
 // shards and the read-only <C> pass.
@@ -417,6 +418,14 @@ static int tile_cut_tables(fq_ctx* ctx, const GraphPrep& g, int N,
     const i64 ntiles = 1ll << (N - kTileBits);
     const size_t per = (size_t)ntiles * kTcutStride * wt;
     const size_t need = per * plan.size();
+    // Built for these weights (no upload since) and this N: reuse them, as
+    // an optimiser's calls on one graph do.
+    if (ctx->d_tcut && need <= ctx->tcut_bytes && ctx->tcut_version == ctx->g_version &&
+        ctx->tcut_n == N) {
+        for (size_t i = 0; i < plan.size(); i++) tabs[i] = (char*)ctx->d_tcut + i * per;
+        return FQ_OK;
+    }
+    ctx->tcut_version = -1;
     if (need > ctx->tcut_bytes) {
         if (ctx->d_tcut) {
             FQ_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -458,6 +467,8 @@ static int tile_cut_tables(fq_ctx* ctx, const GraphPrep& g, int N,
             (const double*)ctx->d_w, N, G, ntiles, (double*)ctx->d_tcut);
     FQ_CUDA(cudaGetLastError());
     ctx->launches++;
+    ctx->tcut_version = ctx->g_version;
+    ctx->tcut_n = N;
     for (size_t i = 0; i < plan.size(); i++) tabs[i] = (char*)ctx->d_tcut + i * per;
     return FQ_OK;
 }

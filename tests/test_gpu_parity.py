@@ -221,6 +221,38 @@ def test_fused_forward_vs_oracle(ctx, oracle, n, P, kind):
         st.free()
 
 
+def test_tile_cut_tables_follow_graph_and_size(fq):
+    """The per-tile cut tables a context keeps between calls are rebuilt when
+    the weights or N change: every call matches a fresh context bit for bit,
+    whatever ran on the context before it."""
+    rng = np.random.default_rng(77)
+    graphs = {21: [complete_int(21, rng), gnp_fp(21, rng)], 22: [complete_int(22, rng)]}
+    g, b = angles(rng, 3)
+    order = [(21, 0), (21, 0), (21, 1), (22, 0), (21, 0), (21, 1), (21, 1)]
+    fresh = {}
+    for n, i in set(order):
+        c = fq.Context(0)
+        try:
+            st = c.state(n)
+            e = c.qaoa_forward(st, graphs[n][i], g, b, energy=True)
+            fresh[(n, i)] = (st.to_host(), e)
+            st.free()
+        finally:
+            c.close()
+    c = fq.Context(0)
+    try:
+        for n, i in order:
+            st = c.state(n)
+            e = c.qaoa_forward(st, graphs[n][i], g, b, energy=True)
+            got = st.to_host()
+            st.free()
+            want, ew = fresh[(n, i)]
+            assert np.array_equal(got, want), (n, i)
+            assert e == ew, (n, i)
+    finally:
+        c.close()
+
+
 @pytest.mark.parametrize("beta", [0.0, np.pi / 2 - 1e-9, 2.5, np.pi, 4.0, -1.0, 7.0])
 def test_fused_forward_mixer_angle_range(ctx, oracle, beta):
     """Both reduced-gate forms (tan and cot) and angles outside [0, pi/2)."""
