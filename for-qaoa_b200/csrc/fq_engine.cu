@@ -736,7 +736,7 @@ namespace fq {
 // RX(angle) (full form, src/rx.cu:47-50) on every qubit of `mask`: qubits
 // below 12 share the contiguous tile, higher ones are covered by strided
 // tiles of up to 9 qubits.
-static int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double angle) {
+int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double angle) {
     const double s = sin(angle / 2), c = cos(angle / 2);  // src/rx.cu:121
     if (!mask) return FQ_OK;
     if (N < kTileBits) {

@@ -49,6 +49,8 @@ int reduce_to_result(fq_ctx* ctx, int n);
 // Copies ctx->d_result[0] to *host (synchronises).
 int read_result(fq_ctx* ctx, double* host);
 int check_state(void* sv, int N);
+// RX(angle) (full form) on every qubit whose bit is set in mask (fq_rx_targets).
+int rx_mask(fq_ctx* ctx, void* sv, int N, unsigned long long mask, double angle);
 int setup_graph(fq_ctx* ctx, const double* graph, int N, GraphPrep& g);
 // The forward circuit (fq_qaoa_forward); skip_last stops before the last
 // pass of the last layer (the gradient's turnaround pass runs it).

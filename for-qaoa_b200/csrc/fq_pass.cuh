@@ -99,6 +99,12 @@ struct PassArgs {
     double f2b;      // fused adjoint passes: f^2 of the earlier layer's gate (A.gx2)
     int pf_dist;     // prefetch the tile pf_dist grid-strides ahead into L2 (0 = off)
     i64 goff;        // shard of a larger state: global index of sv[0] (enters cut values only)
+    // Non-fused PH_MUL passes: RX (full form, pc = cos, ps = sin of angle/2)
+    // on the layout-L0 register bits pre_mask (tile bits 8..11) of each
+    // loaded tile before the phase; a shard's exchange brings the qubits it
+    // swaps in to those bits of the next layer's first pass (0 = none).
+    unsigned pre_mask;
+    double pc, ps;
     // Cut constants of every tile of this pass's geometry, kTcutStride WT per
     // tile (K, then e_0..e_11; k_tile_cuts), or null: each tile computes its
     // own (CutTables::tile, warps 0 and 1, then a barrier).
@@ -861,6 +867,9 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
 #pragma unroll
             for (int r = 0; r < kRegs; r++) __stcs(p + off0(r), v[r]);
             continue;
+        }
+        if constexpr (PH == PH_MUL && !FUSED) {
+            if (A.pre_mask) rx_regs<GM_FULL>(v, A.pre_mask, 0.0, A.pc, A.ps);
         }
         if (PH != PH_NONE && !FUSED) apply_phase(L0t(), cbase, g0, g1, g2, g3);
         // Final layout: L1 after an exchange (<C> then takes the cut

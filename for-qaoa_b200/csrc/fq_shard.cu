@@ -41,24 +41,34 @@ PassArgs shard_args(fq_ctx* ctx, void* sv, int N, int D, int rank, const GraphPr
     return A;
 }
 
-}  // namespace
-
-extern "C" {
-
-int fq_shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank, const double* graph,
-                   double gamma, double beta, int first_layer) {
+// One layer on a shard; pre != nullptr: first RX(*pre) on local qubits
+// n-D..n-1, inside the first pass when its tile holds them in tile bits
+// 8..11 (the layout-L0 register bits), else as a pass of its own.
+int shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank, const double* graph,
+                double gamma, double beta, int first_layer, const double* pre) {
     FQ_TRY(validate_ctx(ctx));
     FQ_TRY(check_shard(shard, N, D, rank));
     FQ_CHECK(isfinite(gamma) && isfinite(beta), FQ_ERR_INVALID, "non-finite angle");
+    FQ_CHECK(!pre || isfinite(*pre), FQ_ERR_INVALID, "non-finite angle");
     GraphPrep g;
     FQ_TRY(setup_graph(ctx, graph, N, g));
     const int n = N - D;
     const std::vector<PassPlan> plan = plan_layer(n);
+    unsigned pre_mask = 0;
+    if (pre) {
+        const PassPlan& f = plan[0];
+        const int k = kTileBits - f.l;  // the first pass's strided targets: qubits a..a+k-1
+        if (D <= 4 && f.l < kTileBits && f.a + k == n && k >= D)
+            pre_mask = ((1u << D) - 1) << (4 - D);  // tile bits 12-D..11 = qubits n-D..n-1
+        else
+            FQ_TRY(rx_mask(ctx, shard, n, ((1ull << D) - 1) << (n - D), *pre));
+    }
     int gm;
     double gx, f;
     gate_params(beta, gm, gx, f);
     // The reduced gates of the n local qubits are folded into the phase; the
-    // D top qubits are rotated later in full form (fq_rx_targets).
+    // D top qubits are rotated later in full form (fq_rx_targets, or the
+    // next layer's first pass).
     const double scale = pow(f, n) * (first_layer ? fq_init_amp(N) : 1.0);
     const int nhi = g.integer ? engine_nhi(g) : 0;
     if (g.integer) {
@@ -77,12 +87,31 @@ int fq_shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank, const doubl
         A.tree = phase_tree_ok(g, gamma) ? 1 : 0;
         A.gamma = gamma;
         A.scale = g.integer ? 1.0 : scale;
+        if (i == 0 && pre_mask) {  // the formula and operand order of rx_mask's passes
+            A.pre_mask = pre_mask;
+            A.pc = cos(*pre / 2);
+            A.ps = sin(*pre / 2);
+        }
         if (i == 0)
             FQ_TRY(dispatch_phase_pass(ctx, g.integer, first_layer ? PH_INIT : PH_MUL, gm, A));
         else
             FQ_TRY(dispatch_rx(ctx, g.integer, gm, false, A));
     }
     return FQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fq_shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank, const double* graph,
+                   double gamma, double beta, int first_layer) {
+    return shard_layer(ctx, shard, N, D, rank, graph, gamma, beta, first_layer, nullptr);
+}
+
+int fq_shard_layer_after_swap(fq_ctx* ctx, void* shard, int N, int D, int rank,
+                              const double* graph, double gamma, double beta, double beta_prev) {
+    return shard_layer(ctx, shard, N, D, rank, graph, gamma, beta, 0, &beta_prev);
 }
 
 int fq_shard_expectation(fq_ctx* ctx, const void* shard, int N, int D, int rank,

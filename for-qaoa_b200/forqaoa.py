@@ -62,6 +62,7 @@ SIGNATURES = {
     "fq_swap_blocks": (_i, [_vp, _vp, _i, _i, _i, _i]),
     "fq_relabel_graph": (_i, [_dp, _i, _i, _i, _i]),
     "fq_shard_layer": (_i, [_vp, _vp, _i, _i, _i, _dp, _d, _d, _i]),
+    "fq_shard_layer_after_swap": (_i, [_vp, _vp, _i, _i, _i, _dp, _d, _d, _d]),
     "fq_shard_expectation": (_i, [_vp, _vp, _i, _i, _i, _dp, _dp]),
     "fq_qaoa_forward": (_i, [_vp, _vp, _i, _i, _dp, _dp, _dp, _dp]),
     "fq_expectation": (_i, [_vp, _vp, _i, _dp, _dp]),
@@ -273,6 +274,15 @@ class Context:
         g = _f64(graph)
         _check(_lib.fq_shard_layer(self.handle, _vp(ptr), N, D, rank, _dptr(g), gamma, beta,
                                    int(bool(first_layer))), "fq_shard_layer")
+
+    def shard_layer_after_swap(self, ptr, N, D, rank, graph, gamma, beta, beta_prev):
+        """RX(beta_prev) on the qubits the last all-to-all swapped in
+        (local qubits N-2D..N-D-1), then a later layer on shard `rank`
+        (fq_shard_layer_after_swap: the rotation inside the layer's first
+        pass where its tile allows)."""
+        g = _f64(graph)
+        _check(_lib.fq_shard_layer_after_swap(self.handle, _vp(ptr), N, D, rank, _dptr(g), gamma,
+                                              beta, beta_prev), "fq_shard_layer_after_swap")
 
     def shard_expectation(self, ptr, N, D, rank, graph):
         """This shard's part of <C> (fq_shard_expectation)."""

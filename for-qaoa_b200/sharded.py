@@ -14,7 +14,9 @@ The state of N qubits is split by its top D index bits: rank r holds the
      [N-D, N) -- the reference's global/local swap (src/swap.cu:223-345),
      here with no packing kernel because the chunks are contiguous;
   3. every rank: RX(beta) on qubits N-2D..N-D-1, which now hold the qubits
-     that were global (fq_rx_targets);
+     that were global: inside the next layer's first pass
+     (fq_shard_layer_after_swap, one sweep fewer per layer), after the last
+     layer as a pass of its own (fq_rx_targets);
   4. the graph is relabelled for the new physical order (fq_relabel_graph,
      as mapping_after_swap_conti, src/swap.cu:27-50) and the label map
      records which logical qubit each physical position holds.
@@ -59,6 +61,10 @@ class ShardOps:
     def layer(self, graph, gamma, beta, first_layer):
         self.ctx.shard_layer(self.buf.data_ptr(), self.N, self.D, self.rank, graph, gamma, beta,
                              first_layer)
+
+    def layer_after_swap(self, graph, gamma, beta, beta_prev):
+        self.ctx.shard_layer_after_swap(self.buf.data_ptr(), self.N, self.D, self.rank, graph,
+                                        gamma, beta, beta_prev)
 
     def rx_top(self, beta):
         n, D = self.n, self.D
@@ -111,19 +117,25 @@ def relabel(graph, swap_out, swap_in, k):
     return forqaoa.relabel_graph(graph, swap_out, swap_in, k)
 
 
-def forward(shards, exchange, N, D, graph, gammas, betas, relabel_fn=relabel):
+def forward(shards, exchange, N, D, graph, gammas, betas, relabel_fn=relabel, fuse=True):
     """The P-layer circuit from |+>^N on the given shards.  Returns the
     label map (physical position -> logical qubit) and the graph in the
-    final physical order."""
+    final physical order.  fuse: rotate the qubits each all-to-all swaps in
+    inside the next layer's first pass (`layer_after_swap`) instead of in a
+    pass of their own (`rx_top`) after every exchange."""
     n = N - D
     labels = np.arange(N)
     g = np.ascontiguousarray(graph, dtype=np.float64)
     for p, (gamma, beta) in enumerate(zip(gammas, betas)):
         for s in shards:
-            s.layer(g, gamma, beta, p == 0)
+            if p > 0 and fuse:
+                s.layer_after_swap(g, gamma, beta, betas[p - 1])
+            else:
+                s.layer(g, gamma, beta, p == 0)
         exchange(shards)
-        for s in shards:
-            s.rx_top(beta)
+        if not fuse or p == len(gammas) - 1:
+            for s in shards:
+                s.rx_top(beta)
         g = relabel_fn(g, n - D, n, D)
         labels[n - D:n], labels[n:N] = labels[n:N].copy(), labels[n - D:n].copy()
     return labels, g
@@ -142,10 +154,13 @@ def to_logical(state_phys, labels):
     return out
 
 
-def emulate(n_qubits, D, P, seed):
+def emulate(n_qubits, D, P, seed, fuse=True):
     """Every shard on GPU 0 (the exchange as chunk copies): device time per
-    layer of the shard passes, the exchange and the RX of the swapped-in
-    qubits, by CUDA events (the first layer runs untimed as warm-up)."""
+    layer of the shard passes, the exchange and the separate RX passes of
+    the swapped-in qubits, by CUDA events (one layer runs untimed first as
+    warm-up).  With `fuse` the swapped-in qubits are rotated inside the
+    next layer's first pass, and only the last layer's are a pass of their
+    own."""
     import torch
     rng = np.random.default_rng(seed)
     N = n_qubits
@@ -163,19 +178,26 @@ def emulate(n_qubits, D, P, seed):
             e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             e[0].record(stream)
             for s in shards:
-                s.layer(gphys, g[p], b[p], p == 0)
+                if p > 0 and fuse:
+                    s.layer_after_swap(gphys, g[p], b[p], b[p - 1])
+                else:
+                    s.layer(gphys, g[p], b[p], p == 0)
             e[1].record(stream)
             local_exchange(shards)
             e[2].record(stream)
-            for s in shards:
-                s.rx_top(b[p])
+            if not fuse or p == P - 1:
+                for s in shards:
+                    s.rx_top(b[p])
             e[3].record(stream)
             torch.cuda.synchronize()
             for k, (i, j) in zip(t, ((0, 1), (1, 2), (2, 3))):
                 t[k] += e[i].elapsed_time(e[j])
             gphys = relabel(gphys, n - D, n, D)
+        ms = {k: v / P for k, v in t.items()}
         return {"N": N, "D": D, "p": P, "shards_on_one_gpu": 1 << D,
-                "ms_per_layer": {k: v / P for k, v in t.items()}}
+                "schedule": "swapped-in RX in the next layer's first pass" if fuse
+                else "swapped-in RX as a pass of its own",
+                "ms_per_layer": ms, "ms_per_layer_total": sum(ms.values())}
     finally:
         ctx.close()
 
@@ -190,9 +212,11 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--emulate", type=int, default=0, metavar="D",
                     help="run all 2^D shards on GPU 0 (no torch.distributed) and time the parts")
+    ap.add_argument("--no-fuse", action="store_true",
+                    help="rotate the swapped-in qubits in a pass of their own after every exchange")
     a = ap.parse_args(argv)
     if a.emulate:
-        print(json.dumps(emulate(a.n, a.emulate, a.p, a.seed)))
+        print(json.dumps(emulate(a.n, a.emulate, a.p, a.seed, fuse=not a.no_fuse)))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -213,7 +237,7 @@ def main(argv=None):
         torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        _, g = forward([s], dist_exchange, a.n, D, W, gammas, betas)
+        _, g = forward([s], dist_exchange, a.n, D, W, gammas, betas, fuse=not a.no_fuse)
         t1.record(stream)
         torch.cuda.synchronize()
         times.append(t0.elapsed_time(t1) / 1000.0)

@@ -146,6 +146,16 @@ int fq_relabel_graph(double* graph_upper, int N, int swap_out, int swap_in,
  * RX(beta) on the shard's local qubits 0..N-D-1. */
 int fq_shard_layer(fq_ctx* ctx, void* shard, int N, int D, int rank,
                    const double* graph_upper, double gamma, double beta, int first_layer);
+/* RX(beta_prev) on local qubits N-2D..N-D-1 (the qubits the previous
+ * layer's all-to-all swapped in), then fq_shard_layer with first_layer = 0:
+ * the same result as fq_rx_targets followed by fq_shard_layer.  For D <= 4
+ * and N-D >= 24 (the layer's first pass then tiles the top local qubits)
+ * the rotation runs inside that pass, one HBM sweep fewer per layer; a
+ * P-layer circuit then calls fq_shard_layer once, this function P-1 times,
+ * and fq_rx_targets once after the last all-to-all. */
+int fq_shard_layer_after_swap(fq_ctx* ctx, void* shard, int N, int D, int rank,
+                              const double* graph_upper, double gamma, double beta,
+                              double beta_prev);
 /* <C> summed over this shard's amplitudes (the shards' partials add up to
  * <C>); synchronises the stream. */
 int fq_shard_expectation(fq_ctx* ctx, const void* shard, int N, int D, int rank,

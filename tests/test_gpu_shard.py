@@ -1,6 +1,6 @@
 """GPU parity of the sharded (D > 0) path: every shard of the state on this
-one GPU, the passes through the C ABI (fq_shard_layer, fq_rx_targets,
-fq_shard_expectation), the all-to-all as chunk copies (`local_exchange`,
+one GPU, the passes through the C ABI (fq_shard_layer,
+fq_shard_layer_after_swap, fq_rx_targets, fq_shard_expectation), the all-to-all as chunk copies (`local_exchange`,
 the same data movement `dist_exchange` does across GPUs), the schedule of
 for-qaoa_b200/sharded.py.  The gathered state, in logical order by the
 label map, and the summed <C> are checked against the oracle, and at
@@ -17,18 +17,18 @@ pytestmark = pytest.mark.gpu
 sys.path.insert(0, PKG)
 
 
-def run_sharded(fq, N, D, W, g, b):
+def run_sharded(fq, N, D, W, g, b, fuse=True, logical=True):
     import torch
     import sharded
     prev = torch.cuda.current_stream()
     stream, ctx = sharded.shard_context(0)
     try:
         shards = [sharded.ShardOps(ctx, N, D, r, "cuda") for r in range(1 << D)]
-        labels, gfin = sharded.forward(shards, sharded.local_exchange, N, D, W, g, b)
+        labels, gfin = sharded.forward(shards, sharded.local_exchange, N, D, W, g, b, fuse=fuse)
         e = sum(s.expectation(gfin) for s in shards)
         psi = torch.cat([s.buf for s in shards]).cpu().numpy()
         torch.cuda.synchronize()
-        return sharded.to_logical(psi, labels), e
+        return (sharded.to_logical(psi, labels) if logical else psi), e
     finally:
         ctx.close()
         torch.cuda.set_stream(prev)
@@ -67,6 +67,44 @@ def test_sharded_matches_engine_n24(fq, ctx):
     finally:
         st.free()
     assert_state_close(psi, want, what="sharded N=24 D=2 vs engine")
+    assert abs(e - ef) <= ENERGY_RTOL * abs(ef)
+
+
+@pytest.mark.parametrize("N,D,P,kind", [
+    (25, 1, 3, "int"), (26, 2, 2, "fp"), (26, 1, 2, "huge"), (28, 4, 2, "int"), (27, 3, 3, "neg"),
+])
+def test_swapped_in_rx_inside_first_pass(fq, N, D, P, kind):
+    """fq_shard_layer_after_swap rotates the swapped-in qubits inside the
+    layer's first pass (N-D >= 24, D <= 4): the same state as the rotation
+    in a pass of its own after each exchange, bit for bit with one
+    swapped-in qubit (the same formula on the same operands), within
+    rounding with several (their order differs)."""
+    rng = np.random.default_rng(17 * N + D)
+    W = graph(kind, N, rng)
+    g, b = angles(rng, P)
+    # Both schedules leave the same label map: compare in physical order.
+    psi_f, e_f = run_sharded(fq, N, D, W, g, b, fuse=True, logical=False)
+    psi_s, e_s = run_sharded(fq, N, D, W, g, b, fuse=False, logical=False)
+    if D == 1:
+        assert np.array_equal(psi_f, psi_s)
+    else:
+        assert_state_close(psi_f, psi_s, what=f"fused vs separate N={N} D={D}")
+    assert abs(e_f - e_s) <= ENERGY_RTOL * abs(e_s)
+
+
+def test_sharded_fused_schedule_matches_engine_n26(fq, ctx):
+    rng = np.random.default_rng(2626)
+    N, D, P = 26, 2, 4
+    W = complete_int(N, rng)
+    g, b = angles(rng, P)
+    psi, e = run_sharded(fq, N, D, W, g, b, fuse=True)
+    st = ctx.state(N)
+    try:
+        ef = ctx.qaoa_forward(st, W, g, b)
+        want = st.to_host()
+    finally:
+        st.free()
+    assert_state_close(psi, want, what="sharded N=26 D=2 (fused) vs engine")
     assert abs(e - ef) <= ENERGY_RTOL * abs(ef)
 
 

@@ -59,6 +59,10 @@ class NumpyShard:
         for q in range(self.n):
             self._rx(psi, q, beta)
 
+    def layer_after_swap(self, graph, gamma, beta, beta_prev):
+        self.rx_top(beta_prev)
+        self.layer(graph, gamma, beta, False)
+
     def rx_top(self, beta):
         psi = self.buf.numpy()
         for q in range(self.n - self.D, self.n):
@@ -118,16 +122,18 @@ def test_sharded_schedule_matches_oracle(oracle, world, N, P, kind):
     assert sorted(labels.tolist()) == list(range(N))
 
 
+@pytest.mark.parametrize("fuse", [True, False])
 @pytest.mark.parametrize("D,N,P", [(1, 8, 2), (2, 9, 3), (3, 10, 2)])
-def test_local_exchange_schedule_matches_oracle(oracle, D, N, P):
+def test_local_exchange_schedule_matches_oracle(oracle, D, N, P, fuse):
     """Every shard in this process: `local_exchange` (the chunk copies the
-    one-GPU emulation uses) in place of the collective."""
+    one-GPU emulation uses) in place of the collective; the swapped-in
+    qubits rotated in the next layer's first pass or after each exchange."""
     import sharded
     rng = np.random.default_rng(7 * N + D)
     W = complete_int(N, rng)
     g, b = angles(rng, P)
     shards = [NumpyShard(N, D, r) for r in range(1 << D)]
-    labels, gfin = sharded.forward(shards, sharded.local_exchange, N, D, W, g, b)
+    labels, gfin = sharded.forward(shards, sharded.local_exchange, N, D, W, g, b, fuse=fuse)
     psi = torch.cat([s.buf for s in shards]).numpy()
     want = oracle.qaoa_logical(W, g, b)
     assert_state_close(sharded.to_logical(psi, labels), want, what=f"local N={N} D={D}")
