@@ -4,8 +4,8 @@
 namespace fq {
 
 int dispatch_dual_phase_fp(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
-                           double* gg, double* gb2) {
-    return dual_phase_dispatch<double>(ctx, gm, gm2, A, gb, gg, gb2);
+                           double* gg, double* gb2, bool store) {
+    return dual_phase_dispatch<double>(ctx, gm, gm2, A, gb, gg, gb2, store);
 }
 
 int dispatch_dual_turn_fp(fq_ctx* ctx, int gm, int gmf, const PassArgs& A, double* gb,

@@ -286,8 +286,12 @@ int grad_enqueue(fq_ctx* ctx, void* sv, void* costate, int N, int P, const doubl
                 A.f2b = f[k - 1] * f[k - 1];
                 rotated[k - 1] += nt;
             }
-            FQ_TRY(g.integer ? dispatch_dual_phase_int(ctx, gm[k], gm2, A, gb, gg, gb2)
-                             : dispatch_dual_phase_fp(ctx, gm[k], gm2, A, gb, gg, gb2));
+            // Layer 0's completing pass ends the sweep: psi and lambda are
+            // workspaces whose final contents nothing reads, so it only
+            // reads them (32 instead of 64 B per amplitude).
+            const bool store = q + 1 < nrev;
+            FQ_TRY(g.integer ? dispatch_dual_phase_int(ctx, gm[k], gm2, A, gb, gg, gb2, store)
+                             : dispatch_dual_phase_fp(ctx, gm[k], gm2, A, gb, gg, gb2, store));
         }
         const bool energy_here = turn && q == 0;  // <C> partials of the turnaround
         if (batched) {

@@ -215,10 +215,11 @@ inline int dispatch_fused(fq_ctx* ctx, bool integer, int gm1, int gm2, const Pas
 // RX(-beta) (gm, A.gx) on A.tmask, dE/dgamma and the inverse phase, then
 // with gm2 != GM_NONE the earlier layer's RX(-beta) (gm2, A.gx2) on A.tmask.
 // Partials: gb (beta), gg (gamma), gb2 (the earlier layer's beta).
+// store = false (gm2 == GM_NONE only) leaves both vectors unwritten.
 int dispatch_dual_phase_int(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
-                            double* gg, double* gb2);
+                            double* gg, double* gb2, bool store = true);
 int dispatch_dual_phase_fp(fq_ctx* ctx, int gm, int gm2, const PassArgs& A, double* gb,
-                           double* gg, double* gb2);
+                           double* gg, double* gb2, bool store = true);
 // The gradient's turnaround (k_pass_dual with TURN): the forward's last pass
 // (gmf, A.gx2), lambda = C psi with <C> (partials to ge), and the reverse
 // sweep's first pass (gm, A.gx; dE/dbeta partials to gb), in one sweep.
