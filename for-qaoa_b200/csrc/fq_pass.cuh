@@ -326,7 +326,7 @@ __device__ __forceinline__ void exchange(double2 (&v)[kRegs], double2* buf, int 
 // barrier keeps a partner's slots unwritten until both lanes have read them,
 // whatever the caller writes next.  On B200 at N=30 the layer-0 pass takes
 // 5.16-5.29 ms with it against 5.39-5.42 with rx_lane; the fused passes
-// measured no faster with it and keep rx_lane (A/B in one call).
+// measured no faster with it (A/B in one call) and use exchange_lanet.
 template <int LF, int LT, int GM, bool PAIR = false>
 __device__ __forceinline__ void exchange_lane(double2 (&v)[kRegs], double2* buf, int tid,
                                               bool wait_readers, int grp, int j, double g,
@@ -344,6 +344,48 @@ __device__ __forceinline__ void exchange_lane(double2 (&v)[kRegs], double2* buf,
         v[r] = rx_self<GM>(rb[o], qb[o], g, c, s);
     }
     __syncwarp();
+}
+
+// exchange<LF, LT> preceded by RX on the qubit of lane bit j, with half of
+// rx_lane's shuffles: the two lanes of a pair (lane bit j = 0, 1) trade the
+// registers whose bit 0 differs from their lane bit (8 values each way),
+// after which each register pair (r, r|1) holds the lane qubit's two
+// amplitudes of one register index and is rotated in place, by rx_lane's
+// own arithmetic.  Every value then goes to the slot of the thread and
+// register that held it before the trade.  A partner's slots written here
+// are those whose values it has just sent, so its reads of them are done:
+// the leading-barrier rule of exchange holds as before.  On B200 at N=30,
+// p=5: fused passes 8.82-8.86 against 8.94-9.02 ms with rx_lane, 65.0-65.3
+// against 64.4-64.6 layers/s (A/B in one call, bit-identical states).
+template <int LF, int LT, int GM, bool PAIR = false>
+__device__ __forceinline__ void exchange_lanet(double2 (&v)[kRegs], double2* buf, int tid,
+                                               bool wait_readers, int grp, int j, double g,
+                                               double c, double s) {
+    const unsigned lm = 1u << j;
+    const bool hi = (tid >> j) & 1;
+#pragma unroll
+    for (int r = 0; r < kRegs; r += 2) {
+        const double2 keep = hi ? v[r | 1] : v[r], send = hi ? v[r] : v[r | 1];
+        double2 q;
+        q.x = __shfl_xor_sync(0xffffffffu, send.x, lm);
+        q.y = __shfl_xor_sync(0xffffffffu, send.y, lm);
+        v[r] = rx_self<GM>(keep, q, g, c, s);      // this lane's amplitude of register r|hi
+        v[r | 1] = rx_self<GM>(q, keep, g, c, s);  // the partner's
+    }
+    if (wait_readers) buf_sync<LF, LT, PAIR>(grp);
+    const int d = hi ? pslot(lay_index<LF>(0, 1)) : 0;
+    double2* const wk = buf + pbase<LF>(tid) + d;
+    double2* const wp = buf + pbase<LF>(tid ^ (int)lm) + d;
+#pragma unroll
+    for (int r = 0; r < kRegs; r += 2) {
+        const int o = pslot(lay_index<LF>(0, r));
+        wk[o] = v[r];
+        wp[o] = v[r | 1];
+    }
+    buf_sync<LF, LT, PAIR>(grp);
+    const double2* const rb = buf + pbase<LT>(tid);
+#pragma unroll
+    for (int r = 0; r < kRegs; r++) v[r] = rb[pslot(lay_index<LT>(0, r))];
 }
 
 constexpr int kWfStride = 21;  // row stride of the compact weight tables (odd: no bank conflicts)
@@ -837,7 +879,7 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
         auto rx_rounds = [&](auto gm_tag, double gx, bool first) {
             constexpr int G = decltype(gm_tag)::value;
             rx_regs<G>(v, m_hi, gx, A.c, A.s);
-            if ((SC == SC_L0 || GM2 != GM_NONE) && lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
+            if (SC == SC_L0 && lo_lane >= 0) rx_lane<G>(v, lo_lane, gx, A.c, A.s);
             if (SC == SC_L021) {
                 exchange<0, 2, PAIR>(v, buf, tid, !(first && skip_lead), grp);
                 rx_regs<G>(v, m_lo, gx, A.c, A.s);
@@ -846,6 +888,9 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
                 if (GM2 == GM_NONE && lo_lane >= 0)
                     exchange_lane<0, 1, G, PAIR>(v, buf, tid, !(first && skip_lead), grp, lo_lane, gx,
                                                  A.c, A.s);
+                else if (lo_lane >= 0)
+                    exchange_lanet<0, 1, G, PAIR>(v, buf, tid, !(first && skip_lead), grp, lo_lane,
+                                                  gx, A.c, A.s);
                 else
                     exchange<0, 1, PAIR>(v, buf, tid, !(first && skip_lead), grp);
             }
@@ -894,13 +939,15 @@ __global__ void __launch_bounds__(PAIR ? 2 * kPassThreads : kPassThreads, PAIR ?
                     ct.template consts<1>(kp, tid, cb, h0, h1, h2, h3);
                     apply_phase(L1t(), cb, h0, h1, h2, h3);
                     rx_regs<G2>(v, m_mid, A.gx2, A.c, A.s);
-                    // A single target among tile bits 0..3 is a lane bit in L1
-                    // as in L0.
-                    if (lo_lane >= 0) rx_lane<G2>(v, lo_lane, A.gx2, A.c, A.s);
                     if (SC == SC_L021) {
                         exchange<1, 2, PAIR>(v, buf, tid, false, grp);
                         rx_regs<G2>(v, m_lo, A.gx2, A.c, A.s);
                         exchange<2, 0, PAIR>(v, buf, tid, false, grp);
+                    } else if (lo_lane >= 0) {
+                        // A single target among tile bits 0..3 is a lane bit
+                        // in L1 as in L0.
+                        exchange_lanet<1, 0, G2, PAIR>(v, buf, tid, false, grp, lo_lane, A.gx2,
+                                                       A.c, A.s);
                     } else {
                         exchange<1, 0, PAIR>(v, buf, tid, false, grp);
                     }
