@@ -205,6 +205,9 @@ def test_fused_engine_vs_golden(ctx, fq, path):
     (2, 1, "int"), (3, 2, "fp"), (7, 3, "neg"), (11, 2, "int"), (12, 1, "int"), (12, 3, "fp"),
     (13, 2, "neg"), (16, 4, "int"), (17, 2, "sparse"), (20, 3, "fp"), (21, 2, "int"),
     (22, 2, "int"), (14, 2, "wide"), (15, 2, "huge"), (16, 1, "zero"),
+    # paired strided tiles with FP64 weights (phases from products of
+    # exponentials): rows of 4 (N=22) and 2 (N=23) amplitudes
+    (22, 3, "fp"), (23, 2, "fp"), (23, 3, "huge"),
 ])
 def test_fused_forward_vs_oracle(ctx, oracle, n, P, kind):
     rng = np.random.default_rng(n * 13 + P)
