@@ -128,3 +128,5 @@ def test_shard_arguments_rejected(fq, ctx):
     W = np.triu(np.ones((14, 14)), 1)
     with pytest.raises(fq.FQError):   # rank outside [0, 2^D)
         ctx.shard_layer(buf.data_ptr(), 14, 1, 2, W, 0.3, 0.2, True)
+    with pytest.raises(fq.FQError):   # non-finite angle of the swapped-in qubits
+        ctx.shard_layer_after_swap(buf.data_ptr(), 14, 1, 0, W, 0.3, 0.2, float("nan"))
