@@ -17,14 +17,17 @@
 // Thread layout: 256 threads x 16 amplitudes in registers.  The 16 register
 // slots of a thread are 4 tile bits; RX on those 4 qubits is register-local.
 // Three layouts rotate which 4 tile bits are register bits; moving between
-// them goes through a 64 KB shared buffer with an XOR swizzle that keeps
-// every quarter-warp's 16-byte accesses in distinct banks:
+// them goes through a shared buffer padded by one slot every 16 (pslot: 68
+// KB per tile), which keeps every quarter-warp's 16-byte accesses in
+// distinct banks in all three layouts:
 //   L0 (load):       regs = tile bits 8..11, lanes = 0..4,  warps = 5..7
 //   L1 (store):      regs = tile bits 4..7,  lanes = 0..3,8, warps = 9..11
 //   L2:              regs = tile bits 0..3,  lanes = 4..8,  warps = 9..11
 // L0 and L1 both keep the row bits on consecutive lanes, so a tile is loaded
 // in L0 and stored from L1 without a layout change of its own: 12 qubits
-// take two exchanges (L0 -> L2 -> L1), 8 take one (L0 -> L1).  A single
+// take two exchanges (L0 -> L2 -> L1), 8 take one (L0 -> L1).  Passes that
+// alternate (ALT, ALTM) load their odd tiles in L1 and store them from L0
+// instead.  A single
 // qubit among tile bits 0..3 is rotated with warp shuffles instead (those
 // bits are lane bits in L0 and L1), so a strided pass with 128-byte rows
 // (9 qubits, tile bits 3..11) also needs one exchange.
@@ -250,8 +253,9 @@ __device__ __forceinline__ void group_sync(int g) {
 }
 
 // Layouts L1 and L2 both put tile bits 9..11 on the warp index, so a change
-// between them stays inside each warp's 512-amplitude region of buf (the
-// swizzle only permutes bits 0..2): a warp barrier is enough.  Such an
+// between them stays inside each warp's 512-amplitude region of buf
+// (neither the padding nor the TMA pass's swizzle, which permutes bits 0..2,
+// moves a slot out of it): a warp barrier is enough.  Such an
 // exchange must follow reads of buf in L1 or L2 (the warp's own region), as
 // every schedule here does; exchanges from or to L0 cross warps and use the
 // block barrier.
