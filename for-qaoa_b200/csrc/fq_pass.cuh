@@ -26,11 +26,10 @@
 // L0 and L1 both keep the row bits on consecutive lanes, so a tile is loaded
 // in L0 and stored from L1 without a layout change of its own: 12 qubits
 // take two exchanges (L0 -> L2 -> L1), 8 take one (L0 -> L1).  Passes that
-// alternate (ALT, ALTM) load their odd tiles in L1 and store them from L0
-// instead.  A single
-// qubit among tile bits 0..3 is rotated with warp shuffles instead (those
-// bits are lane bits in L0 and L1), so a strided pass with 128-byte rows
-// (9 qubits, tile bits 3..11) also needs one exchange.
+// alternate (ALT, ALTM) load their odd tiles in L1 and store them from L0.
+// A single qubit among tile bits 0..3 is rotated with warp shuffles instead
+// (those bits are lane bits in L0 and L1), so a strided pass with 128-byte
+// rows (9 qubits, tile bits 3..11) also needs one exchange.
 //
 // Cut value of an amplitude (exact in integers for integer weights):
 //   C(z) = K(fixed) + C_TT(tile bits) + sum_{u in tile} z_u e_u(fixed)
